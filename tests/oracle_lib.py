@@ -1,0 +1,382 @@
+"""ctypes bindings to the CPU oracle (oracle/_build/liboracle.so).
+
+Test infrastructure: the parity checker for the CUDA path and the CPU baseline.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+ORACLE_SO = ROOT / "oracle" / "_build" / "liboracle.so"
+REF_SO = ROOT / "oracle" / "_ref" / "libvortex_ref.so"
+P = 0x7FFFFFFF
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not ORACLE_SO.exists():
+            build()
+        _lib = C.CDLL(str(ORACLE_SO))
+        _declare(_lib)
+    return _lib
+
+
+u32p = C.POINTER(C.c_uint32)
+u64p = C.POINTER(C.c_uint64)
+u8p = C.POINTER(C.c_uint8)
+
+
+def _declare(L: C.CDLL) -> None:
+    L.oracle_prove.restype = C.c_uint64
+    L.oracle_ch_draw_number.restype = C.c_uint64
+    L.oracle_m31_mul.restype = C.c_uint32
+    L.oracle_m31_inv.restype = C.c_uint32
+    L.oracle_bench_commit.restype = C.c_double
+    L.oracle_bench_fri.restype = C.c_double
+    L.oracle_verify.restype = C.c_int
+
+
+def ptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    if a.dtype == np.uint32:
+        return a.ctypes.data_as(u32p)
+    if a.dtype == np.uint64:
+        return a.ctypes.data_as(u64p)
+    if a.dtype == np.uint8:
+        return a.ctypes.data_as(u8p)
+    raise TypeError(a.dtype)
+
+
+def ptr_array(arrs):
+    """A C array of uint32_t* pointing at the given numpy arrays."""
+    return (u32p * len(arrs))(*[ptr(a) for a in arrs])
+
+
+# ----------------------------------------------------------------- field / circle
+def coset(kind: int, log_n: int):
+    o = np.zeros(4, np.uint32)
+    lib().oracle_coset(kind, log_n, ptr(o))
+    return [int(x) for x in o]
+
+
+HALF_COSET, HALF_ODDS, SUBGROUP = 0, 1, 2
+
+
+def seeded_m31(seed: int, n: int, offset: int = 0) -> np.ndarray:
+    o = np.empty(n, np.uint32)
+    lib().oracle_seeded_m31(C.c_uint64(seed), C.c_uint64(offset), C.c_uint64(n), ptr(o))
+    return o
+
+
+# ----------------------------------------------------------------- NTT
+def native_twiddles(log_n: int, kind: int = HALF_COSET):
+    n = 1 << log_n
+    line = np.zeros(n - 1, np.uint32)
+    iline = np.zeros(n - 1, np.uint32)
+    circ = np.zeros(n // 2, np.uint32)
+    icirc = np.zeros(n // 2, np.uint32)
+    offs = np.zeros(max(log_n - 1, 1), np.uint32)
+    sizes = np.zeros(max(log_n - 1, 1), np.uint32)
+    lib().oracle_native_twiddles(kind, log_n, ptr(line), ptr(circ), ptr(iline), ptr(icirc), ptr(offs), ptr(sizes))
+    return dict(line=line, circle=circ, iline=iline, icircle=icirc, offsets=offs[: log_n - 1], sizes=sizes[: log_n - 1])
+
+
+def native_evaluate(d: np.ndarray, log_n: int) -> np.ndarray:
+    d = np.ascontiguousarray(d, np.uint32).copy()
+    lib().oracle_native_evaluate(ptr(d), log_n)
+    return d
+
+
+def native_interpolate(d: np.ndarray, log_n: int) -> np.ndarray:
+    d = np.ascontiguousarray(d, np.uint32).copy()
+    lib().oracle_native_interpolate(ptr(d), log_n)
+    return d
+
+
+def ntt_layer(d: np.ndarray, tw: np.ndarray, layer_idx: int, forward: bool) -> np.ndarray:
+    d = np.ascontiguousarray(d, np.uint32).copy()
+    lib().oracle_ntt_layer(ptr(d), C.c_uint64(d.size), ptr(np.ascontiguousarray(tw, np.uint32)), layer_idx, int(forward))
+    return d
+
+
+def stwo_twiddles(log_n: int):
+    n = 1 << log_n
+    f = np.zeros(n // 2, np.uint32)
+    i = np.zeros(n // 2, np.uint32)
+    lib().oracle_stwo_twiddles(log_n, ptr(f), ptr(i))
+    return f, i
+
+
+def stwo_evaluate(d: np.ndarray, log_n: int) -> np.ndarray:
+    d = np.ascontiguousarray(d, np.uint32).copy()
+    lib().oracle_stwo_evaluate(ptr(d), log_n)
+    return d
+
+
+def stwo_interpolate(d: np.ndarray, log_n: int) -> np.ndarray:
+    d = np.ascontiguousarray(d, np.uint32).copy()
+    lib().oracle_stwo_interpolate(ptr(d), log_n)
+    return d
+
+
+def stwo_lde_columns(cols: np.ndarray, log_n: int, blowup: int = 2, threads: int = 1) -> np.ndarray:
+    cols = np.ascontiguousarray(cols, np.uint32)
+    nc = cols.shape[0]
+    out = np.empty((nc, 1 << (log_n + blowup)), np.uint32)
+    lib().oracle_stwo_lde_columns(ptr(cols), nc, log_n, blowup, ptr(out), threads)
+    return out
+
+
+def bit_reverse(d: np.ndarray, log_n: int) -> np.ndarray:
+    d = np.ascontiguousarray(d, np.uint32).copy()
+    lib().oracle_bit_reverse(ptr(d), log_n)
+    return d
+
+
+def batch_inverse(x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.uint32)
+    o = np.empty_like(x)
+    lib().oracle_batch_inverse(ptr(x), ptr(o), C.c_uint64(x.size))
+    return o
+
+
+def coset_points(init_x, init_y, step_x, step_y, n):
+    ox = np.empty(n, np.uint32)
+    oy = np.empty(n, np.uint32)
+    lib().oracle_coset_points(init_x, init_y, step_x, step_y, C.c_uint64(n), ptr(ox), ptr(oy))
+    return ox, oy
+
+
+# ----------------------------------------------------------------- hashing / Merkle
+def blake2s_words(w: np.ndarray) -> np.ndarray:
+    w = np.ascontiguousarray(w, np.uint32)
+    o = np.empty(8, np.uint32)
+    lib().oracle_blake2s_words(ptr(w), C.c_uint64(w.size), ptr(o))
+    return o
+
+
+def blake2s_bytes(b: bytes) -> bytes:
+    a = np.frombuffer(b, np.uint8).copy() if b else np.zeros(1, np.uint8)
+    o = np.empty(32, np.uint8)
+    lib().oracle_blake2s_bytes(ptr(a), C.c_uint64(len(b)), ptr(o))
+    return o.tobytes()
+
+
+def leaf_hashes_capped(cols: np.ndarray) -> np.ndarray:
+    cols = np.ascontiguousarray(cols, np.uint32)
+    nc, n = cols.shape
+    o = np.empty((n, 8), np.uint32)
+    lib().oracle_leaf_hashes_capped(ptr(cols), nc, C.c_uint64(n), ptr(o))
+    return o
+
+
+def hash_nodes(children: np.ndarray) -> np.ndarray:
+    children = np.ascontiguousarray(children, np.uint32).reshape(-1)
+    n_par = children.size // 16
+    o = np.empty((n_par, 8), np.uint32)
+    lib().oracle_hash_nodes(ptr(children), C.c_uint64(n_par), ptr(o))
+    return o
+
+
+def merkle_root_hashes(h: np.ndarray) -> np.ndarray:
+    h = np.ascontiguousarray(h, np.uint32)
+    o = np.empty(8, np.uint32)
+    lib().oracle_merkle_root_hashes(ptr(h), C.c_uint64(h.size // 8), ptr(o))
+    return o
+
+
+def merkle_root_capped(cols: np.ndarray, threads: int = 1) -> np.ndarray:
+    cols = np.ascontiguousarray(cols, np.uint32)
+    o = np.empty(8, np.uint32)
+    lib().oracle_merkle_root_capped(ptr(cols), cols.shape[0], C.c_uint64(cols.shape[1]), threads, ptr(o))
+    return o
+
+
+def merkle_root_rowpacked(cols: np.ndarray, threads: int = 1) -> np.ndarray:
+    cols = np.ascontiguousarray(cols, np.uint32)
+    o = np.empty(8, np.uint32)
+    lib().oracle_merkle_root_rowpacked(ptr(cols), cols.shape[0], C.c_uint64(cols.shape[1]), threads, ptr(o))
+    return o
+
+
+def merkle_root_soa4(c: np.ndarray, threads: int = 1) -> np.ndarray:
+    c = np.ascontiguousarray(c, np.uint32)
+    o = np.empty(8, np.uint32)
+    lib().oracle_merkle_root_soa4(ptr(c[0]), ptr(c[1]), ptr(c[2]), ptr(c[3]), C.c_uint64(c.shape[1]), threads, ptr(o))
+    return o
+
+
+def lifted_leaves(cols, col_logs, lifting_log) -> np.ndarray:
+    cols = [np.ascontiguousarray(c, np.uint32) for c in cols]
+    logs = np.asarray(col_logs, np.uint32)
+    o = np.empty((1 << lifting_log, 8), np.uint32)
+    lib().oracle_lifted_leaves(ptr_array(cols), ptr(logs), len(cols), lifting_log, ptr(o))
+    return o
+
+
+# ----------------------------------------------------------------- channel
+class ChState(C.Structure):
+    _fields_ = [("state", C.c_uint8 * 32), ("n_draws", C.c_uint32)]
+
+
+class Channel:
+    def __init__(self):
+        self.s = ChState()
+
+    def mix_digest(self, d):
+        a = np.ascontiguousarray(d, np.uint32)
+        lib().oracle_ch_mix_digest(C.byref(self.s), ptr(a))
+
+    def mix_felts(self, felts):
+        a = np.ascontiguousarray(felts, np.uint32).reshape(-1)
+        lib().oracle_ch_mix_felts(C.byref(self.s), ptr(a), C.c_uint64(a.size // 4))
+
+    def mix_u64(self, v):
+        lib().oracle_ch_mix_u64(C.byref(self.s), C.c_uint64(v))
+
+    def draw_felt(self):
+        o = np.empty(4, np.uint32)
+        lib().oracle_ch_draw_felt(C.byref(self.s), ptr(o))
+        return o
+
+    def draw_number(self, bound):
+        return int(lib().oracle_ch_draw_number(C.byref(self.s), C.c_uint64(bound)))
+
+    def draw_queries(self, log_domain, n):
+        o = np.empty(n, np.uint64)
+        lib().oracle_ch_draw_queries(C.byref(self.s), log_domain, C.c_uint64(n), ptr(o))
+        return o
+
+    def state_bytes(self) -> bytes:
+        return bytes(self.s.state)
+
+    def oods_point(self):
+        o = np.empty(8, np.uint32)
+        lib().oracle_oods_point(C.byref(self.s), ptr(o))
+        return o
+
+
+# ----------------------------------------------------------------- FRI / quotient
+def fold_twiddles(kind: int, log_n: int, extract_y: bool) -> np.ndarray:
+    o = np.empty(1 << (log_n - 1), np.uint32)
+    lib().oracle_fold_twiddles(kind, log_n, int(extract_y), ptr(o))
+    return o
+
+
+def fold_twiddles_generic(ix, iy, sx, sy, log_n, extract_y) -> np.ndarray:
+    o = np.empty(1 << (log_n - 1), np.uint32)
+    lib().oracle_fold_twiddles_generic(ix, iy, sx, sy, log_n, int(extract_y), ptr(o))
+    return o
+
+
+def fold_circle_into_line(dst: np.ndarray, src: np.ndarray, tw, alpha, alpha_sq) -> np.ndarray:
+    dst = np.ascontiguousarray(dst, np.uint32).copy()
+    src = np.ascontiguousarray(src, np.uint32)
+    a = np.asarray(alpha, np.uint32)
+    a2 = np.asarray(alpha_sq, np.uint32)
+    lib().oracle_fold_circle_into_line(ptr_array(list(dst)), ptr_array(list(src)), ptr(np.ascontiguousarray(tw, np.uint32)),
+                                       ptr(a), ptr(a2), C.c_uint64(dst.shape[1]))
+    return dst
+
+
+def fold_line(src: np.ndarray, tw, alpha) -> np.ndarray:
+    src = np.ascontiguousarray(src, np.uint32)
+    out = np.zeros((4, src.shape[1] // 2), np.uint32)
+    a = np.asarray(alpha, np.uint32)
+    lib().oracle_fold_line(ptr_array(list(src)), ptr(np.ascontiguousarray(tw, np.uint32)), ptr_array(list(out)), ptr(a),
+                           C.c_uint64(out.shape[1]))
+    return out
+
+
+def last_layer_poly_coeffs(evals) -> np.ndarray:
+    e = np.ascontiguousarray(evals, np.uint32)
+    o = np.empty((8, 4), np.uint32)
+    lib().oracle_last_layer_poly_coeffs(ptr(e), C.c_uint64(e.shape[0]), ptr(o))
+    return o
+
+
+def eval_last_layer_poly(coeffs, idx, log_size) -> np.ndarray:
+    c = np.ascontiguousarray(coeffs, np.uint32)
+    o = np.empty(4, np.uint32)
+    lib().oracle_eval_last_layer_poly(ptr(c), C.c_uint64(c.shape[0]), C.c_uint64(idx), log_size, ptr(o))
+    return o
+
+
+def fib_quotient(trace: np.ndarray, alpha) -> np.ndarray:
+    trace = np.ascontiguousarray(trace, np.uint32)
+    out = np.zeros((4, trace.size), np.uint32)
+    lib().oracle_fib_quotient(ptr(trace), C.c_uint64(trace.size), ptr(np.asarray(alpha, np.uint32)), ptr_array(list(out)))
+    return out
+
+
+def accumulate_numerators(cols, col_idx, b, c, n_rows) -> np.ndarray:
+    cols = [np.ascontiguousarray(x, np.uint32) for x in cols]
+    out = np.zeros((4, n_rows), np.uint32)
+    lib().oracle_accumulate_numerators(ptr_array(cols), ptr(np.asarray(col_idx, np.uint32)),
+                                       ptr(np.ascontiguousarray(b, np.uint32)), ptr(np.ascontiguousarray(c, np.uint32)),
+                                       len(col_idx), C.c_uint64(n_rows), ptr_array(list(out)))
+    return out
+
+
+def quotients_combine(spx, spy, fla, numers, acc_logs, dxs, dys, lifting_log) -> np.ndarray:
+    n_rows = dxs.size
+    out = np.zeros((4, n_rows), np.uint32)
+    numers = [np.ascontiguousarray(x, np.uint32) for x in numers]
+    n0 = ptr_array([x[0] for x in numers])
+    n1 = ptr_array([x[1] for x in numers])
+    n2 = ptr_array([x[2] for x in numers])
+    n3 = ptr_array([x[3] for x in numers])
+    lib().oracle_quotients_combine(ptr(np.ascontiguousarray(spx, np.uint32)), ptr(np.ascontiguousarray(spy, np.uint32)),
+                                   ptr(np.ascontiguousarray(fla, np.uint32)), n0, n1, n2, n3,
+                                   ptr(np.asarray(acc_logs, np.uint32)), len(numers), ptr(dxs), ptr(dys), lifting_log,
+                                   C.c_uint64(n_rows), ptr_array(list(out)))
+    return out
+
+
+def eval_at_oods(coeffs, z8) -> np.ndarray:
+    c = np.ascontiguousarray(coeffs, np.uint32)
+    o = np.empty(4, np.uint32)
+    lib().oracle_eval_at_oods(ptr(c), C.c_uint64(c.size), ptr(np.ascontiguousarray(z8, np.uint32)), ptr(o))
+    return o
+
+
+def line_coeffs(z8, v):
+    a = np.empty(4, np.uint32)
+    b = np.empty(4, np.uint32)
+    lib().oracle_line_coeffs(ptr(np.ascontiguousarray(z8, np.uint32)), ptr(np.ascontiguousarray(v, np.uint32)), ptr(a), ptr(b))
+    return a, b
+
+
+# ----------------------------------------------------------------- prover
+def fib_trace(a, b, log_n) -> np.ndarray:
+    o = np.empty(1 << log_n, np.uint32)
+    lib().oracle_fib_trace(a, b, log_n, ptr(o))
+    return o
+
+
+def prove(a: int, b: int, log_n: int, threads: int = 0) -> bytes:
+    threads = threads or (os.cpu_count() or 1)
+    n = lib().oracle_prove(a, b, log_n, threads, None, C.c_uint64(0))
+    buf = np.empty(n, np.uint8)
+    lib().oracle_prove(a, b, log_n, threads, ptr(buf), C.c_uint64(n))
+    return buf.tobytes()
+
+
+def verify(proof: bytes):
+    a = np.frombuffer(proof, np.uint8).copy()
+    err = C.create_string_buffer(256)
+    rc = lib().oracle_verify(ptr(a), C.c_uint64(a.size), err, C.c_uint64(256))
+    return rc, err.value.decode()
