@@ -1,0 +1,322 @@
+#!/usr/bin/env python3
+"""Commitment-layer benchmark on B200: committed M31 elements/s.
+
+Workload (one step): 34 columns x 2^24 rows of seeded uniform M31 values, treated
+as bit-reversed canonic evaluations, go through circle interpolation, x4
+low-degree extension (CanonicCoset(26), bit-reversed output) and a row-packed
+Blake2s-256 Merkle root; then one seeded uniform QM31 vector of 2^26 values is
+folded by FRI (circle fold, then line folds down to 8 values) with seeded fold
+challenges, committing every folded layer.
+
+Committed elements per step = 34 * 2^26 (trace LDE leaves) + 4 * (2^26 - 8)
+(the FRI layers' SoA4 leaves).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vstark|reference]
+
+N > 1 runs one independent replica per GPU (weak scaling, no collective on the
+data path); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SEED = 0x56530001
+METRIC = "committed M31 elems/s & proofs/s batched vs plain on 1 B200; p50/p99 latency"
+UNIT = "committed M31 elements/s"
+
+
+def splitmix_m31(seed: int, offset: int, n: int) -> list[int]:
+    """Same stream as vs_fill_uniform_m31 (host side, for the few fold challenges)."""
+    P, M = 0x7FFFFFFF, (1 << 64) - 1
+
+    def at(c):
+        z = (seed + 0x9E3779B97F4A7C15 * c) & M
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        return z ^ (z >> 31)
+
+    out = []
+    for k in range(offset, offset + n):
+        v = at(k + 1) >> 33
+        if v == P:
+            v = at(k + 2) >> 33
+            v = 0 if v == P else v
+        out.append(v)
+    return out
+
+
+def workload(args):
+    n_cols, log_n, blow, fri_log = args.cols, args.log_n, 2, args.fri_log
+    N = 1 << (log_n + blow)
+    committed = n_cols * N + 4 * ((1 << (fri_log - 1)) * 2 - 8)
+    return n_cols, log_n, blow, fri_log, N, committed
+
+
+def config_json(args):
+    n_cols, log_n, blow, fri_log, N, _ = workload(args)
+    return {"workload": f"commitment layer: {n_cols} cols x 2^{log_n} rows, stwo LDE x{1 << blow} + row-packed "
+                        f"Blake2s root, then FRI fold+commit of 2^{fri_log} QM31",
+            "n_cols": n_cols, "log_n": log_n, "blowup": 1 << blow, "fri_log_n": fri_log,
+            "l2": "inputs larger than L2 (2.2 GB columns, 1 GB QM31 vector)", "seed": hex(SEED)}
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.lines, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU (oracle) baseline
+def cpu_sample(args, threads: int):
+    """The oracle's CPU pipeline on a bounded sample of the same workload."""
+    import numpy as np
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as O
+    n_cols, _, blow, _, _, _ = workload(args)
+    s_log, f_log = args.cpu_log_n, args.cpu_log_n + blow
+    cols = O.seeded_m31(SEED, n_cols << s_log).reshape(n_cols, -1)
+    root = np.zeros(8, np.uint32)
+    t_commit = O.lib().oracle_bench_commit(O.ptr(cols), n_cols, s_log, blow, threads, O.ptr(root))
+    src = O.seeded_m31(SEED + 1, 4 << f_log).reshape(4, -1)
+    alphas = np.array(splitmix_m31(SEED + 2, 0, 4 * (f_log - 3)), np.uint32)
+    roots = np.zeros((f_log - 3, 8), np.uint32)
+    last = np.zeros((8, 4), np.uint32)
+    t_fri = O.lib().oracle_bench_fri(O.ptr_array(list(src)), f_log, O.ptr(alphas), threads, O.ptr(roots), O.ptr(last))
+    elems = n_cols * (1 << f_log) + 4 * ((1 << f_log) - 8)
+    secs = t_commit + t_fri
+    return {"value": elems / secs, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n_cols} cols x 2^{s_log} rows (LDE 2^{f_log}) + FRI of 2^{f_log} QM31, "
+                      f"{secs:.2f} s on {threads} threads"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    if not (ROOT / "tests" / "oracle_lib.py").exists():
+        print(json.dumps({"impl": "reference", "unavailable": "CPU oracle sources missing"}))
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(args, threads)
+    vals = [cpu_sample(args, threads) for _ in range(args.steps)]
+    v = statistics.mean(x["value"] for x in vals)
+    _, _, _, _, _, committed = workload(args)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": committed / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31)",
+            "data": "synthetic (seeded SplitMix64 uniform M31)", "config": config_json(args),
+            "cpu_baseline": dict(vals[-1], value=v),
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="vstark", choices=["vstark", "reference"])
+    ap.add_argument("--cols", type=int, default=34)
+    ap.add_argument("--log-n", type=int, default=24)
+    ap.add_argument("--fri-log", type=int, default=26)
+    ap.add_argument("--cpu-log-n", type=int, default=16, help="row log of the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import vortexstark_b200 as V
+    from vortexstark_b200 import api
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    V.lib()  # raises if the CUDA library is missing
+
+    n_cols, log_n, blow, fri_log, N, committed = workload(args)
+    n = 1 << log_n
+    st = torch.cuda.current_stream()
+    cols = torch.empty((n_cols, n), dtype=torch.int32, device="cuda")
+    api.fill_uniform_m31(cols, SEED, offset=rank * (n_cols << log_n))
+    fri_src = torch.empty((4, 1 << fri_log), dtype=torch.int32, device="cuda")
+    api.fill_uniform_m31(fri_src, SEED + 1, offset=rank * (4 << fri_log))
+    alphas = splitmix_m31(SEED + 2, 0, 4 * (fri_log - 3))
+    alphas = [alphas[4 * i:4 * i + 4] for i in range(fri_log - 3)]
+    lde = torch.empty((n_cols, N), dtype=torch.int32, device="cuda")
+    root = torch.zeros(8, dtype=torch.int32, device="cuda")
+    work = torch.empty(4 << fri_log, dtype=torch.int32, device="cuda")
+    roots = torch.zeros(8 * (fri_log - 3), dtype=torch.int32, device="cuda")
+    last = torch.zeros(32, dtype=torch.int32, device="cuda")
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def step(marks=None):
+        if marks is not None:
+            marks[0].record(st)
+        api.lde_stwo(cols, log_n, blow, out=lde)
+        if marks is not None:
+            marks[1].record(st)
+        api.merkle_root_rowpacked(lde, root)
+        if marks is not None:
+            marks[2].record(st)
+        api.fri_fold_commit(fri_src, fri_log, alphas, work, roots, last)
+        if marks is not None:
+            marks[3].record(st)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    marks = [[ev() for _ in range(4)] for _ in range(args.steps)]
+    l0 = api.launch_count()
+    vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    with ClockSampler(vis[local] if local < len(vis) else local) as clk:
+        t0, t1 = ev(), ev()
+        t0.record(st)
+        for k in range(args.steps):
+            step(marks[k])
+        t1.record(st)
+        torch.cuda.synchronize()
+    launches = (api.launch_count() - l0) // args.steps
+    ms = t0.elapsed_time(t1) / args.steps
+    phase = {"lde": 0.0, "merkle": 0.0, "fri": 0.0}
+    for m in marks:
+        phase["lde"] += m[0].elapsed_time(m[1]) / args.steps
+        phase["merkle"] += m[1].elapsed_time(m[2]) / args.steps
+        phase["fri"] += m[2].elapsed_time(m[3]) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = committed * world / (ms / 1e3)
+
+    # end to end through the C ABI from pinned host buffers (H2D inputs, D2H roots)
+    e2e = None
+    if not args.no_e2e:
+        cols_h = torch.empty_like(cols, device="cpu").pin_memory()
+        fri_h = torch.empty_like(fri_src, device="cpu").pin_memory()
+        cols_h.copy_(cols)
+        fri_h.copy_(fri_src)
+        out_h = torch.empty(8 + 8 * (fri_log - 3) + 32, dtype=torch.int32).pin_memory()
+
+        def e2e_step():
+            cols.copy_(cols_h, non_blocking=True)
+            fri_src.copy_(fri_h, non_blocking=True)
+            step()
+            out_h[:8].copy_(root, non_blocking=True)
+            out_h[8:8 + roots.numel()].copy_(roots, non_blocking=True)
+            out_h[8 + roots.numel():].copy_(last, non_blocking=True)
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = ev(), ev()
+        e0.record(st)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": committed * world / (ems / 1e3), "unit": UNIT, "ms_per_step": ems,
+               "h2d_bytes_per_step": (cols.numel() + fri_src.numel()) * 4, "d2h_bytes_per_step": out_h.numel() * 4}
+
+    # roofline of the dominant phase: algorithmic bytes per step / phase time
+    hbm = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0)) \
+        if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
+    alg = {"lde": n_cols * (4 * n + 4 * N), "merkle": n_cols * 4 * N,
+           "fri": sum(24 * (1 << (l - 1)) for l in range(4, fri_log + 1))}
+    dom = max(phase, key=phase.get)
+    ach = alg[dom] / (phase[dom] / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel_phase": dom, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+            "traffic": None, "phase_ms": phase,
+            "phase_hbm_frac": {k: alg[k] / (phase[k] / 1e3) / 1e9 / hbm for k in phase}}
+
+    if rank == 0:
+        cpu = None if args.no_cpu else cpu_sample(args, os.cpu_count() or 1)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic (seeded SplitMix64 uniform M31)",
+                "config": config_json(args), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

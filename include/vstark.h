@@ -1,0 +1,234 @@
+/*
+ * vstark.h — C ABI of libvstark, a B200-native (sm_100a) implementation of the
+ * VortexSTARK polynomial-commitment hot path.
+ *
+ * Two groups of entry points:
+ *
+ * 1. Drop-in symbols with the exact names, argument meaning, ownership and
+ *    synchronisation of the reference's CUDA static library (declared in the
+ *    reference at src/cuda/ffi.rs, defined in cuda/*.cu). Each cites the
+ *    reference declaration it replaces. As in the reference: all pointers are
+ *    device pointers unless named h_* or documented "host"; the caller owns all
+ *    device memory; launches go to the legacy default stream unless a stream is
+ *    passed; functions return void. A failed launch is recorded and can be read
+ *    with vs_last_error() (the reference surfaces it through cudaGetLastError).
+ *
+ * 2. vs_* entry points (no reference counterpart) returning a vs_status, used by
+ *    the batched / served paths and by bench.py.
+ *
+ * All field values are canonical M31 residues (< 2^31 - 1), as in the reference.
+ */
+#ifndef VSTARK_H
+#define VSTARK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* vs_stream_t; /* == cudaStream_t */
+
+enum {
+  VS_OK = 0,
+  VS_ERR_INVALID = 1,  /* bad argument (size not a power of two, null pointer, ...) */
+  VS_ERR_CUDA = 2,     /* CUDA runtime error */
+  VS_ERR_OOM = 3,      /* device allocation failed */
+  VS_ERR_BUDGET = 4,   /* job does not fit the configured HBM budget */
+  VS_ERR_TIMEOUT = 5,  /* a bounded wait gave up */
+  VS_ERR_CANCELLED = 6,
+  VS_ERR_BUSY = 7      /* queue full / retry later */
+};
+
+/* Last error message of the calling thread ("" when none). */
+const char* vs_last_error(void);
+/* Library version string. */
+const char* vs_version(void);
+/* Number of kernels the vs_* entry points of this process have launched so far. */
+uint64_t vs_launch_count(void);
+
+/* ===================================================================== */
+/* 1. Reference-compatible drop-in entry points                           */
+/* ===================================================================== */
+
+/* --- native circle NTT (src/cuda/ffi.rs:243-283; cuda/circle_ntt.cu:181-343) ---
+ * Twiddles in the reference layout: line twiddles concatenated per line layer,
+ * layer l at d_twiddles + h_layer_offsets[l] (host array), circle twiddles
+ * separate. In place; synchronises the device before returning (as the
+ * reference does). */
+void cuda_circle_ntt_evaluate(uint32_t* d_data, const uint32_t* d_twiddles, const uint32_t* d_circle_twids,
+                              const uint32_t* h_layer_offsets, const uint32_t* h_layer_sizes, uint32_t n_line_layers,
+                              uint32_t n);
+void cuda_circle_ntt_interpolate(uint32_t* d_data, const uint32_t* d_itwiddles, const uint32_t* d_circle_itwids,
+                                 const uint32_t* h_layer_offsets, const uint32_t* h_layer_sizes,
+                                 uint32_t n_line_layers, uint32_t n);
+/* d_columns: device array of n_cols device pointers (src/cuda/ffi.rs:263-283). */
+void cuda_circle_ntt_evaluate_batch(uint32_t** d_columns, const uint32_t* d_twiddles, const uint32_t* d_circle_twids,
+                                    const uint32_t* h_layer_offsets, const uint32_t* h_layer_sizes,
+                                    uint32_t n_line_layers, uint32_t n, uint32_t n_cols);
+void cuda_circle_ntt_interpolate_batch(uint32_t** d_columns, const uint32_t* d_itwiddles,
+                                       const uint32_t* d_circle_itwids, const uint32_t* h_layer_offsets,
+                                       const uint32_t* h_layer_sizes, uint32_t n_line_layers, uint32_t n,
+                                       uint32_t n_cols);
+/* One butterfly layer, stride 2^layer_idx (src/cuda/ffi.rs:285-291; circle_ntt.cu:318-333). Async. */
+void cuda_circle_ntt_layer(uint32_t* d_data, const uint32_t* d_twiddles, uint32_t layer_idx, uint32_t n, int forward);
+/* In-place bit reversal of 2^log_n words (src/cuda/ffi.rs:293; circle_ntt.cu:338-343). Async. */
+void cuda_bit_reverse_m31(uint32_t* data, uint32_t log_n);
+/* Evaluate a polynomial at a QM31 point by folding (src/cuda/ffi.rs:295-302; circle_ntt.cu:345-384).
+ * d_folding_factors: log2(n) QM31 factors (4 words each); h_result: host[4]; scratch: 2 x (n/2*4) words. */
+void cuda_eval_at_point(const uint32_t* d_coeffs, const uint32_t* d_folding_factors, uint32_t* h_result, uint32_t n,
+                        uint32_t* d_scratch1, uint32_t* d_scratch2);
+
+/* --- stwo / CanonicCoset NTT (src/cuda/ffi.rs:234-239; cuda/circle_ntt_stwo.cu:268-402) ---
+ * Flat stwo twiddle table of n/2 words (src/ntt.rs:262-325 layout). Output of
+ * evaluate is in bit-reversed canonic order. Synchronises before returning. */
+void cuda_stwo_ntt_evaluate(uint32_t* d_data, const uint32_t* d_twiddles, uint32_t n);
+void cuda_stwo_ntt_interpolate(uint32_t* d_data, const uint32_t* d_itwiddles, uint32_t n);
+
+/* --- twiddles (src/cuda/ffi.rs:327-363; cuda/twiddles.cu, cuda/batch_inverse.cu) --- */
+void cuda_compute_fold_twiddle_sources(uint32_t initial_x, uint32_t initial_y, uint32_t step_x, uint32_t step_y,
+                                       uint32_t* output, uint32_t n, uint32_t log_n, int extract_y);
+void cuda_compute_fold_twiddle_sources_stream(uint32_t initial_x, uint32_t initial_y, uint32_t step_x,
+                                              uint32_t step_y, uint32_t* output, uint32_t n, uint32_t log_n,
+                                              int extract_y, vs_stream_t stream);
+/* Montgomery-trick inverse over 64-element chunks; 0 -> 0, and a chunk whose
+ * first element is 0 comes out all zero (batch_inverse.cu:8-41). */
+void cuda_batch_inverse_m31(const uint32_t* input, uint32_t* output, uint32_t n);
+void cuda_batch_inverse_m31_stream(const uint32_t* input, uint32_t* output, uint32_t n, vs_stream_t stream);
+void cuda_compute_coset_points(uint32_t initial_x, uint32_t initial_y, uint32_t step_x, uint32_t step_y,
+                               uint32_t* output_x, uint32_t* output_y, uint32_t n);
+void cuda_squash_x(const uint32_t* input, uint32_t* output, uint32_t out_n);
+void cuda_extract_and_squash(const uint32_t* input, uint32_t* twiddle_out, uint32_t* squash_out, uint32_t half_n);
+
+/* --- Fibonacci constraint / LDE helpers (src/cuda/ffi.rs:367-398; cuda/constraint.cu:93-165) ---
+ * alpha: host[4] QM31. Outputs are four SoA columns. */
+void cuda_fibonacci_quotient(const uint32_t* trace, uint32_t* out0, uint32_t* out1, uint32_t* out2, uint32_t* out3,
+                             const uint32_t* alpha, uint32_t n);
+void cuda_zero_pad(const uint32_t* src, uint32_t* dst, uint32_t src_n, uint32_t dst_n);
+void cuda_fibonacci_quotient_chunk(const uint32_t* trace, uint32_t* out0, uint32_t* out1, uint32_t* out2,
+                                   uint32_t* out3, const uint32_t* alpha, uint32_t offset, uint32_t chunk_n,
+                                   uint32_t global_n);
+void cuda_fibonacci_quotient_chunk_stream(const uint32_t* trace, uint32_t* out0, uint32_t* out1, uint32_t* out2,
+                                          uint32_t* out3, const uint32_t* alpha, uint32_t offset, uint32_t chunk_n,
+                                          uint32_t global_n, vs_stream_t stream);
+void cuda_interleave_u32(const uint32_t* even, const uint32_t* odd, uint32_t* output, uint32_t half_n);
+
+/* --- FRI folds, SoA QM31 (src/cuda/ffi.rs:305-324; cuda/fri.cu:80-121) ---
+ * alpha, alpha_sq: host[4]. */
+void cuda_fold_line_soa(const uint32_t* in0, const uint32_t* in1, const uint32_t* in2, const uint32_t* in3,
+                        const uint32_t* twiddles, uint32_t* out0, uint32_t* out1, uint32_t* out2, uint32_t* out3,
+                        const uint32_t* alpha, uint32_t half_n);
+void cuda_fold_circle_into_line_soa(uint32_t* dst0, uint32_t* dst1, uint32_t* dst2, uint32_t* dst3,
+                                    const uint32_t* src0, const uint32_t* src1, const uint32_t* src2,
+                                    const uint32_t* src3, const uint32_t* twiddles, const uint32_t* alpha,
+                                    const uint32_t* alpha_sq, uint32_t half_n);
+
+/* --- Blake2s Merkle (src/cuda/ffi.rs:643-697; cuda/blake2s.cu:522-632) ---
+ * Leaf hash of up to 16 columns (t = min(n_cols,16)*4); SoA4 leaf t = 16;
+ * node = Blake2s(left||right). columns: device array of device pointers.
+ * Tiled variants emit one root per 1024-leaf tile. */
+void cuda_merkle_hash_leaves(const uint32_t* const* columns, uint32_t* hashes, uint32_t n_cols, uint32_t n_leaves);
+void cuda_merkle_hash_nodes(const uint32_t* children, uint32_t* parents, uint32_t n_parents);
+void cuda_merkle_reduce_to_root(const uint32_t* nodes, uint32_t* root_out, uint32_t n_nodes);
+void cuda_merkle_commit_small_soa4(const uint32_t* col0, const uint32_t* col1, const uint32_t* col2,
+                                   const uint32_t* col3, uint32_t* root_out, uint32_t n_leaves);
+void cuda_merkle_hash_leaves_merge_soa4(const uint32_t* col0, const uint32_t* col1, const uint32_t* col2,
+                                        const uint32_t* col3, uint32_t* parents, uint32_t n_leaves);
+void cuda_merkle_tiled_soa4(const uint32_t* col0, const uint32_t* col1, const uint32_t* col2, const uint32_t* col3,
+                            uint32_t* subtree_roots, uint32_t n_leaves);
+void cuda_merkle_tiled_soa4_stream(const uint32_t* col0, const uint32_t* col1, const uint32_t* col2,
+                                   const uint32_t* col3, uint32_t* subtree_roots, uint32_t n_leaves,
+                                   vs_stream_t stream);
+void cuda_merkle_tiled_generic(const uint32_t* const* columns, uint32_t* subtree_roots, uint32_t n_cols,
+                               uint32_t n_leaves);
+/* Row-packed multi-block leaf over any number of columns of mixed sizes
+ * (src/cuda/ffi.rs:769-776; cuda/merkle_leaves_lifted.cu:107-122).
+ * schedule: device array of LeafHashChunk { uint32_t col_indices[16]; uint32_t n_cols; uint32_t log_size; }. */
+void cuda_build_leaves_lifted(const uint32_t* const* col_ptrs, const void* schedule, uint32_t n_chunks,
+                              uint32_t lifting_log_size, uint32_t* output_hashes, uint32_t n_leaves);
+
+/* --- OODS / DEEP quotient (src/cuda/ffi.rs:850-898; cuda/quotient.cu:199-251) --- */
+void cuda_accumulate_numerators(const uint32_t* const* col_ptrs, const uint32_t* col_indices, const uint32_t* b_coeffs,
+                                const uint32_t* c_coeffs, uint32_t n_batch_cols, uint32_t n_rows, uint32_t* out0,
+                                uint32_t* out1, uint32_t* out2, uint32_t* out3);
+void cuda_compute_quotients_combine(const uint32_t* sample_points_x, const uint32_t* sample_points_y,
+                                    const uint32_t* first_linear_acc, const uint32_t* const* numer_ptrs0,
+                                    const uint32_t* const* numer_ptrs1, const uint32_t* const* numer_ptrs2,
+                                    const uint32_t* const* numer_ptrs3, const uint32_t* acc_log_sizes,
+                                    uint32_t n_accs, const uint32_t* domain_xs, const uint32_t* domain_ys,
+                                    uint32_t lifting_log_size, uint32_t n_rows, uint32_t* out0, uint32_t* out1,
+                                    uint32_t* out2, uint32_t* out3);
+
+/* --- misc (src/cuda/ffi.rs:203-207, 946; cuda/fields.cu, cuda/bit_reverse_wide.cu) --- */
+void cuda_bit_reverse_qm31(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t log_n);
+void cuda_m31_add(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n);
+void cuda_m31_mul(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n);
+void cuda_device_sync(void);
+
+/* ===================================================================== */
+/* 2. vs_* entry points (no reference counterpart)                        */
+/* ===================================================================== */
+
+/* Fill `n` words with the seeded uniform-M31 stream used by the benchmarks:
+ * word k = splitmix64(seed + (k+1+offset)*0x9E3779B97F4A7C15) >> 33, re-drawn once
+ * from counter k+2+offset when it equals 2^31-1 (0 if that is 2^31-1 too). */
+int vs_fill_uniform_m31(uint32_t* d_out, uint64_t n, uint64_t seed, uint64_t offset, vs_stream_t stream);
+
+/* Fused LDE in the stwo / CanonicCoset convention: for each of n_cols columns
+ * (column c at d_src + c*src_stride, 2^log_n BRT-canonic evaluations) compute
+ * interpolate -> zero-pad -> evaluate on CanonicCoset(log_n + blowup_bits),
+ * writing column c at d_dst + c*dst_stride (bit-reversed canonic order).
+ * Equivalent to the reference's interpolate_stwo / cuda_zero_pad /
+ * evaluate_stwo chain (src/cairo_air/prover.rs:954-965) without materialising
+ * the zero padding. d_src is not modified. Twiddles are cached per size. */
+int vs_lde_stwo(const uint32_t* d_src, uint64_t src_stride, uint32_t* d_dst, uint64_t dst_stride, uint32_t n_cols,
+                uint32_t log_n, uint32_t blowup_bits, vs_stream_t stream);
+/* Same for the native half_coset convention (src/prover.rs:1745-1762). */
+int vs_lde_native(const uint32_t* d_src, uint64_t src_stride, uint32_t* d_dst, uint64_t dst_stride, uint32_t n_cols,
+                  uint32_t log_n, uint32_t blowup_bits, vs_stream_t stream);
+
+/* Merkle root over n_cols columns of 2^log_leaves rows with the row-packed
+ * multi-block leaf (all columns, merkle_leaves_lifted.cu semantics with equal
+ * sizes). Column c at d_cols + c*stride. root written to d_root (device, 8 words). */
+int vs_merkle_root_rowpacked(const uint32_t* d_cols, uint64_t stride, uint32_t n_cols, uint32_t log_leaves,
+                             uint32_t* d_root, vs_stream_t stream);
+/* Merkle root with the reference's <=16-column leaf (blake2s.cu leaf semantics). */
+int vs_merkle_root_capped(const uint32_t* d_cols, uint64_t stride, uint32_t n_cols, uint32_t log_leaves,
+                          uint32_t* d_root, vs_stream_t stream);
+/* Merkle root of a SoA4 QM31 column (leaf t = 16). */
+int vs_merkle_root_soa4(const uint32_t* d_c0, const uint32_t* d_c1, const uint32_t* d_c2, const uint32_t* d_c3,
+                        uint32_t log_leaves, uint32_t* d_root, vs_stream_t stream);
+
+/* Commitment-layer step: LDE (stwo convention) of n_cols columns of 2^log_n
+ * rows into d_lde (n_cols x 2^(log_n+blowup), column-major), then the
+ * row-packed Blake2s Merkle root into d_root (device, 8 words). */
+int vs_commit_columns(const uint32_t* d_cols, uint32_t n_cols, uint32_t log_n, uint32_t blowup_bits, uint32_t* d_lde,
+                      uint32_t* d_root, vs_stream_t stream);
+
+/* FRI chain on one QM31 evaluation vector (SoA4 in d_src, 4 planes of 2^log_n
+ * words at d_src + k*2^log_n): circle fold on half_coset(log_n), then line folds
+ * on half_odds down to 2^3 values, committing every folded layer (SoA4 leaf).
+ * h_alphas: host, (log_n - 3) QM31 fold challenges. d_work: device scratch of
+ * 4 * 2^log_n words. Writes (log_n - 3) roots (8 words each) to d_roots and the
+ * 8 last-layer QM31 values (AoS) to d_last. */
+int vs_fri_fold_commit(const uint32_t* d_src, uint32_t log_n, const uint32_t* h_alphas, uint32_t* d_work,
+                       uint32_t* d_roots, uint32_t* d_last, vs_stream_t stream);
+
+/* Fibonacci prover (src/prover.rs:192-209 prove(); stage order of
+ * prove_with_cache, src/prover.rs:1721-1978). Writes the proof in the KRAK v1
+ * wire format (src/bin/stark_cli.rs:907-976) into h_out (host) when cap is large
+ * enough; *out_len receives the proof length. */
+int vs_prove_fib(uint32_t a, uint32_t b, uint32_t log_n, uint8_t* h_out, uint64_t cap, uint64_t* out_len,
+                 vs_stream_t stream);
+/* Verifier (src/verifier.rs:39-236) over a KRAK proof. Returns VS_OK when
+ * accepted, VS_ERR_INVALID otherwise with the reason in err (host). */
+int vs_verify_fib(const uint8_t* h_proof, uint64_t len, char* err, uint64_t err_cap);
+
+/* Release cached twiddles and scratch of the current device. */
+int vs_release_caches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VSTARK_H */

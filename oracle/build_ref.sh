@@ -22,6 +22,6 @@ for s in $SRCS; do
   nvcc -O3 -std=c++17 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC -c "$REF_ROOT/cuda/$s" -o "$o"
   OBJS="$OBJS $o"
 done
-nvcc -shared -gencode arch=compute_100a,code=sm_100a $OBJS -o "$OUT/libvortex_ref.so" -lcudart
+nvcc -shared -cudart static -gencode arch=compute_100a,code=sm_100a $OBJS -o "$OUT/libvortex_ref.so"
 rm -f $OBJS
 echo "built $OUT/libvortex_ref.so"

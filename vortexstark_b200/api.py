@@ -1,0 +1,82 @@
+"""Host API over libvstark for torch device tensors.
+
+Names follow the reference's host API for this path: commitment of columns
+(src/merkle.rs commit_root_only / cairo_air trace commit), FRI fold + commit
+(src/fri.rs), Fibonacci prove / verify (src/prover.rs:192, src/verifier.rs:39).
+Tensors are int32 views of u32 field words, on a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import check, lib
+
+PROOF_CAP = 32 << 20  # bytes; the largest proof (log_n = 28) is a few MB
+
+
+def _stream(stream=None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def _ptr(t: torch.Tensor) -> int:
+    if not t.is_cuda or t.dtype != torch.int32 or not t.is_contiguous():
+        raise TypeError("expected a contiguous int32 CUDA tensor")
+    return t.data_ptr()
+
+
+def fill_uniform_m31(out: torch.Tensor, seed: int, offset: int = 0, stream=None) -> torch.Tensor:
+    check(lib().vs_fill_uniform_m31(_ptr(out), out.numel(), seed, offset, _stream(stream)), "vs_fill_uniform_m31")
+    return out
+
+
+def lde_stwo(cols: torch.Tensor, log_n: int, blowup: int = 2, out: torch.Tensor | None = None, stream=None):
+    """cols: (n_cols, 2^log_n) BRT-canonic evaluations -> (n_cols, 2^(log_n+blowup))."""
+    n_cols = cols.shape[0]
+    N = 1 << (log_n + blowup)
+    if out is None:
+        out = torch.empty((n_cols, N), dtype=torch.int32, device=cols.device)
+    check(lib().vs_lde_stwo(_ptr(cols), 1 << log_n, _ptr(out), N, n_cols, log_n, blowup, _stream(stream)), "vs_lde_stwo")
+    return out
+
+
+def commit_columns(cols: torch.Tensor, log_n: int, blowup: int, lde: torch.Tensor, root: torch.Tensor, stream=None):
+    """Commitment-layer step: stwo LDE of every column + row-packed Blake2s Merkle root."""
+    check(lib().vs_commit_columns(_ptr(cols), cols.shape[0], log_n, blowup, _ptr(lde), _ptr(root), _stream(stream)),
+          "vs_commit_columns")
+
+
+def merkle_root_rowpacked(cols: torch.Tensor, root: torch.Tensor, stream=None):
+    n_cols, n = cols.shape
+    check(lib().vs_merkle_root_rowpacked(_ptr(cols), n, n_cols, n.bit_length() - 1, _ptr(root), _stream(stream)),
+          "vs_merkle_root_rowpacked")
+
+
+def fri_fold_commit(src: torch.Tensor, log_n: int, alphas, work: torch.Tensor, roots: torch.Tensor,
+                    last: torch.Tensor, stream=None):
+    """src: (4, 2^log_n) SoA4 QM31; alphas: (log_n - 3) x 4 host words."""
+    flat = [int(x) for row in alphas for x in row]
+    arr = (C.c_uint32 * len(flat))(*flat)
+    check(lib().vs_fri_fold_commit(_ptr(src), log_n, arr, _ptr(work), _ptr(roots), _ptr(last), _stream(stream)),
+          "vs_fri_fold_commit")
+
+
+def prove_fib(a: int, b: int, log_n: int, stream=None) -> bytes:
+    """Fibonacci proof in the KRAK v1 wire format."""
+    buf = (C.c_uint8 * PROOF_CAP)()
+    n = C.c_uint64(0)
+    check(lib().vs_prove_fib(a, b, log_n, buf, PROOF_CAP, C.byref(n), _stream(stream)), "vs_prove_fib")
+    return bytes(buf[: n.value])
+
+
+def verify_fib(proof: bytes) -> tuple[bool, str]:
+    buf = (C.c_uint8 * max(1, len(proof))).from_buffer_copy(proof or b"\0")
+    err = C.create_string_buffer(256)
+    rc = lib().vs_verify_fib(buf, len(proof), err, 256)
+    return rc == 0, err.value.decode()
+
+
+def launch_count() -> int:
+    return int(lib().vs_launch_count())

@@ -1,0 +1,66 @@
+// Host-side Merkle helpers over the generic subtree kernel (merkle_impl.cuh).
+// Templates live here so other translation units can commit with fused leaf
+// functors (FRI folds, constraint quotients).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "merkle_impl.cuh"
+#include "vs_common.cuh"
+
+namespace vs {
+
+// One level of parents: parents[i] = Blake2s(children[2i] || children[2i+1]).
+int launch_hash_nodes(const uint32_t* children, uint32_t* parents, uint64_t n_parents, cudaStream_t st);
+
+template <class Leaf>
+int merkle_tile_roots(const Leaf& leaf, uint64_t n_leaves, uint32_t TL, uint32_t* roots, cudaStream_t st) {
+  const unsigned smem = merkle_smem_bytes(TL);
+  if (smem > 48 * 1024)
+    VS_CUDA(cudaFuncSetAttribute(merkle_subtree_kernel<Leaf>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const uint64_t tiles = (n_leaves + (1ull << TL) - 1) >> TL;
+  merkle_subtree_kernel<Leaf><<<(unsigned)tiles, MK_THREADS, smem, st>>>(leaf, TL, n_leaves, roots);
+  VS_LAUNCHED("merkle_subtree_kernel");
+  return VS_OK;
+}
+
+// Words of scratch merkle_root needs for n_leaves leaves (0 when n_leaves <= 1024).
+inline uint64_t merkle_scratch_words(uint64_t n_leaves) {
+  uint64_t words = 0;
+  for (uint64_t cur = n_leaves >> MK_MAX_TL; n_leaves > (1ull << MK_MAX_TL) && cur > 1; cur >>= MK_MAX_TL) {
+    words += cur * 8;
+    if (cur <= (1ull << MK_MAX_TL)) break;
+  }
+  return words;
+}
+
+// Root of a power-of-two tree whose leaves come from `leaf`. Intermediate tile
+// roots go to `scratch` (merkle_scratch_words(n_leaves) words; when null it is
+// allocated stream-ordered for the call). Each reduction level is written after
+// the previous one, never in place.
+template <class Leaf>
+int merkle_root(const Leaf& leaf, uint64_t n_leaves, uint32_t* d_root, cudaStream_t st, uint32_t* scratch = nullptr) {
+  if (!is_pow2(n_leaves)) return set_error(VS_ERR_INVALID, "merkle: leaf count %llu is not a power of two",
+                                           (unsigned long long)n_leaves);
+  const uint32_t L = ilog2(n_leaves);
+  if (L <= MK_MAX_TL) return merkle_tile_roots(leaf, n_leaves, L, d_root, st);
+  uint32_t* buf = scratch;
+  if (!buf) VS_CUDA(cudaMallocAsync((void**)&buf, merkle_scratch_words(n_leaves) * 4, st));
+  uint64_t cur = n_leaves >> MK_MAX_TL;
+  int rc = merkle_tile_roots(leaf, n_leaves, MK_MAX_TL, buf, st);
+  uint32_t* level = buf;
+  while (rc == VS_OK) {
+    const uint32_t Lc = ilog2(cur);
+    if (Lc <= MK_MAX_TL) { rc = merkle_tile_roots(LeafHashes{level}, cur, Lc, d_root, st); break; }
+    uint32_t* next = level + cur * 8;
+    rc = merkle_tile_roots(LeafHashes{level}, cur, MK_MAX_TL, next, st);
+    level = next;
+    cur >>= MK_MAX_TL;
+  }
+  if (!scratch) {
+    cudaError_t e = cudaFreeAsync(buf, st);
+    if (rc == VS_OK) rc = check_cuda(e, "merkle scratch free");
+  }
+  return rc;
+}
+
+}  // namespace vs

@@ -1,0 +1,188 @@
+// Constraint and OODS quotient kernels: drop-in for cuda/constraint.cu and
+// cuda/quotient.cu, plus the elementwise helpers of cuda/fields.cu.
+#include "vs_common.cuh"
+#include "vs_field.cuh"
+
+namespace vs {
+
+// q[i] = alpha * (t[(i+2)%n] - (t[(i+1)%n] + t[i]))   (constraint.cu:10-64)
+__global__ void fib_quotient_kernel(const uint32_t* __restrict__ t, uint32_t* __restrict__ o0, uint32_t* __restrict__ o1,
+                                    uint32_t* __restrict__ o2, uint32_t* __restrict__ o3, qm31 alpha, uint32_t offset,
+                                    uint32_t chunk_n, uint32_t global_n) {
+  uint32_t li = blockIdx.x * blockDim.x + threadIdx.x;
+  if (li >= chunk_n) return;
+  uint32_t i = offset + li;
+  uint32_t i1 = i + 1 == global_n ? 0 : i + 1;
+  uint32_t i2 = i1 + 1 == global_n ? 0 : i1 + 1;
+  uint32_t c = sub(t[i2], add(t[i1], t[i]));
+  qm31 r = qscale(alpha, c);
+  o0[li] = r.v[0];
+  o1[li] = r.v[1];
+  o2[li] = r.v[2];
+  o3[li] = r.v[3];
+}
+
+__global__ void zero_pad_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint32_t src_n,
+                                uint32_t dst_n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < dst_n) dst[i] = i < src_n ? src[i] : 0u;
+}
+__global__ void interleave_kernel(const uint32_t* __restrict__ e, const uint32_t* __restrict__ o,
+                                  uint32_t* __restrict__ out, uint32_t half_n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < half_n) *reinterpret_cast<uint2*>(out + 2 * (uint64_t)i) = make_uint2(e[i], o[i]);
+}
+
+// numer[row] = sum_i (c_i * f_i[row] - b_i)   (quotient.cu:25-68)
+__global__ void accumulate_numerators_kernel(const uint32_t* const* __restrict__ cols, const uint32_t* __restrict__ idx,
+                                             const uint32_t* __restrict__ b, const uint32_t* __restrict__ c,
+                                             uint32_t n_batch, uint32_t n_rows, uint32_t* __restrict__ o0,
+                                             uint32_t* __restrict__ o1, uint32_t* __restrict__ o2,
+                                             uint32_t* __restrict__ o3) {
+  uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n_rows) return;
+  qm31 acc = qzero();
+  for (uint32_t k = 0; k < n_batch; k++) {
+    uint32_t f = cols[idx[k]][row];
+    qm31 ck{{__ldg(c + 4 * k), __ldg(c + 4 * k + 1), __ldg(c + 4 * k + 2), __ldg(c + 4 * k + 3)}};
+    qm31 bk{{__ldg(b + 4 * k), __ldg(b + 4 * k + 1), __ldg(b + 4 * k + 2), __ldg(b + 4 * k + 3)}};
+    acc = qadd(acc, qsub(qscale(ck, f), bk));
+  }
+  o0[row] = acc.v[0];
+  o1[row] = acc.v[1];
+  o2[row] = acc.v[2];
+  o3[row] = acc.v[3];
+}
+
+// q[row] = sum_j (numer_j[lift(row)] - A_j * y) * D_j(row)^-1 with
+// D = (Re sx - x) Im sy - (Re sy - y) Im sx in CM31   (quotient.cu:101-197)
+__global__ void quotients_combine_kernel(const uint32_t* __restrict__ spx, const uint32_t* __restrict__ spy,
+                                         const uint32_t* __restrict__ fla, const uint32_t* const* __restrict__ n0,
+                                         const uint32_t* const* __restrict__ n1, const uint32_t* const* __restrict__ n2,
+                                         const uint32_t* const* __restrict__ n3, const uint32_t* __restrict__ acc_log,
+                                         uint32_t n_accs, const uint32_t* __restrict__ dxs,
+                                         const uint32_t* __restrict__ dys, uint32_t lifting_log, uint32_t n_rows,
+                                         uint32_t* __restrict__ o0, uint32_t* __restrict__ o1,
+                                         uint32_t* __restrict__ o2, uint32_t* __restrict__ o3) {
+  uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n_rows) return;
+  const uint32_t dx = dxs[row], dy = dys[row];
+  qm31 q = qzero();
+  for (uint32_t j = 0; j < n_accs; j++) {
+    cm31 prx{spx[4 * j], spx[4 * j + 1]}, pix{spx[4 * j + 2], spx[4 * j + 3]};
+    cm31 pry{spy[4 * j], spy[4 * j + 1]}, piy{spy[4 * j + 2], spy[4 * j + 3]};
+    cm31 den = csub(cmul(csub(prx, cm31{dx, 0}), piy), cmul(csub(pry, cm31{dy, 0}), pix));
+    cm31 di = cinv(den);
+    uint32_t ratio = lifting_log - acc_log[j];
+    uint32_t li = ((row >> (ratio + 1)) << 1) + (row & 1);
+    qm31 pn{{n0[j][li], n1[j][li], n2[j][li], n3[j][li]}};
+    qm31 a{{fla[4 * j], fla[4 * j + 1], fla[4 * j + 2], fla[4 * j + 3]}};
+    q = qadd(q, qscale_c(qsub(pn, qscale(a, dy)), di));
+  }
+  o0[row] = q.v[0];
+  o1[row] = q.v[1];
+  o2[row] = q.v[2];
+  o3[row] = q.v[3];
+}
+
+__global__ void m31_binop_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                                 uint32_t* __restrict__ out, uint32_t n, int is_mul) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = is_mul ? mul(a[i], b[i]) : add(a[i], b[i]);
+}
+
+// SplitMix64 counter stream -> uniform M31 (see vs_fill_uniform_m31).
+__device__ __forceinline__ uint64_t splitmix_at(uint64_t seed, uint64_t counter) {
+  uint64_t z = seed + 0x9E3779B97F4A7C15ull * counter;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__global__ void fill_uniform_kernel(uint32_t* __restrict__ out, uint64_t n, uint64_t seed, uint64_t offset) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (; i < n; i += stride) {
+    uint64_t k = offset + i;
+    uint32_t v = (uint32_t)(splitmix_at(seed, k + 1) >> 33);
+    if (v == VS_P) {
+      v = (uint32_t)(splitmix_at(seed, k + 2) >> 33);
+      if (v == VS_P) v = 0;
+    }
+    out[i] = v;
+  }
+}
+
+}  // namespace vs
+
+using namespace vs;
+
+extern "C" {
+
+void cuda_fibonacci_quotient_chunk_stream(const uint32_t* trace, uint32_t* o0, uint32_t* o1, uint32_t* o2, uint32_t* o3,
+                                          const uint32_t* alpha, uint32_t offset, uint32_t chunk_n, uint32_t global_n,
+                                          vs_stream_t stream) {
+  if (!chunk_n) return;
+  fib_quotient_kernel<<<blocks_for(chunk_n, 256), 256, 0, (cudaStream_t)stream>>>(
+      trace, o0, o1, o2, o3, qm31{{alpha[0], alpha[1], alpha[2], alpha[3]}}, offset, chunk_n, global_n);
+  check_cuda(cudaGetLastError(), "cuda_fibonacci_quotient");
+}
+void cuda_fibonacci_quotient_chunk(const uint32_t* trace, uint32_t* o0, uint32_t* o1, uint32_t* o2, uint32_t* o3,
+                                   const uint32_t* alpha, uint32_t offset, uint32_t chunk_n, uint32_t global_n) {
+  cuda_fibonacci_quotient_chunk_stream(trace, o0, o1, o2, o3, alpha, offset, chunk_n, global_n, 0);
+}
+void cuda_fibonacci_quotient(const uint32_t* trace, uint32_t* o0, uint32_t* o1, uint32_t* o2, uint32_t* o3,
+                             const uint32_t* alpha, uint32_t n) {
+  cuda_fibonacci_quotient_chunk_stream(trace, o0, o1, o2, o3, alpha, 0, n, n, 0);
+}
+void cuda_zero_pad(const uint32_t* src, uint32_t* dst, uint32_t src_n, uint32_t dst_n) {
+  if (!dst_n) return;
+  zero_pad_kernel<<<blocks_for(dst_n, 256), 256>>>(src, dst, src_n, dst_n);
+  check_cuda(cudaGetLastError(), "cuda_zero_pad");
+}
+void cuda_interleave_u32(const uint32_t* even, const uint32_t* odd, uint32_t* out, uint32_t half_n) {
+  if (!half_n) return;
+  interleave_kernel<<<blocks_for(half_n, 256), 256>>>(even, odd, out, half_n);
+  check_cuda(cudaGetLastError(), "cuda_interleave_u32");
+}
+void cuda_accumulate_numerators(const uint32_t* const* cols, const uint32_t* idx, const uint32_t* b, const uint32_t* c,
+                                uint32_t n_batch, uint32_t n_rows, uint32_t* o0, uint32_t* o1, uint32_t* o2,
+                                uint32_t* o3) {
+  if (!n_rows) return;
+  accumulate_numerators_kernel<<<blocks_for(n_rows, 256), 256>>>(cols, idx, b, c, n_batch, n_rows, o0, o1, o2, o3);
+  check_cuda(cudaGetLastError(), "cuda_accumulate_numerators");
+}
+void cuda_compute_quotients_combine(const uint32_t* spx, const uint32_t* spy, const uint32_t* fla,
+                                    const uint32_t* const* n0, const uint32_t* const* n1, const uint32_t* const* n2,
+                                    const uint32_t* const* n3, const uint32_t* acc_log, uint32_t n_accs,
+                                    const uint32_t* dxs, const uint32_t* dys, uint32_t lifting_log, uint32_t n_rows,
+                                    uint32_t* o0, uint32_t* o1, uint32_t* o2, uint32_t* o3) {
+  if (!n_rows) return;
+  quotients_combine_kernel<<<blocks_for(n_rows, 256), 256>>>(spx, spy, fla, n0, n1, n2, n3, acc_log, n_accs, dxs, dys,
+                                                             lifting_log, n_rows, o0, o1, o2, o3);
+  check_cuda(cudaGetLastError(), "cuda_compute_quotients_combine");
+}
+void cuda_m31_add(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n) {
+  if (!n) return;
+  m31_binop_kernel<<<blocks_for(n, 256), 256>>>(a, b, out, n, 0);
+  check_cuda(cudaGetLastError(), "cuda_m31_add");
+}
+void cuda_m31_mul(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n) {
+  if (!n) return;
+  m31_binop_kernel<<<blocks_for(n, 256), 256>>>(a, b, out, n, 1);
+  check_cuda(cudaGetLastError(), "cuda_m31_mul");
+}
+void cuda_device_sync(void) { check_cuda(cudaDeviceSynchronize(), "cuda_device_sync"); }
+
+int vs_fill_uniform_m31(uint32_t* d_out, uint64_t n, uint64_t seed, uint64_t offset, vs_stream_t stream) {
+  clear_error();
+  if (!d_out) return set_error(VS_ERR_INVALID, "vs_fill_uniform_m31: null output");
+  if (!n) return VS_OK;
+  unsigned blocks = (unsigned)((n + 255) / 256);
+  unsigned cap = (unsigned)sm_count() * 16;
+  if (blocks > cap) blocks = cap;
+  fill_uniform_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(d_out, n, seed, offset);
+  VS_LAUNCHED("fill_uniform_kernel");
+  return VS_OK;
+}
+
+}  // extern "C"

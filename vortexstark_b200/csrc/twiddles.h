@@ -1,0 +1,45 @@
+// Internal twiddle-table API shared by the NTT, FRI and prover paths.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "vs_field.cuh"
+
+namespace vs {
+
+enum { TW_NATIVE = 0, TW_STWO = 1 };
+enum { COSET_HALF_COSET = 0, COSET_HALF_ODDS = 1, COSET_SUBGROUP = 2 };
+
+struct TwiddleSet {
+  int kind = 0;
+  uint32_t log_n = 0;
+  uint32_t* mem = nullptr;
+  // native: line/iline (n-1 words, reference layout), circle/icircle (n/2)
+  // stwo:   line = forward flat table (n/2), iline = inverse flat table (n/2)
+  uint32_t* line = nullptr;
+  uint32_t* iline = nullptr;
+  uint32_t* circle = nullptr;
+  uint32_t* icircle = nullptr;
+  std::vector<uint32_t> offsets, sizes;  // native per-line-layer (host)
+};
+
+struct HostCoset {
+  cpt initial, step;
+  uint32_t log_size;
+};
+HostCoset host_coset(int which, uint32_t log_size);
+cpt host_repeated_double(cpt p, uint32_t k);
+
+// Cached per (device, kind, log_n); built on the device on first use.
+int get_twiddles(int kind, uint32_t log_n, const TwiddleSet** out, cudaStream_t st);
+// FRI fold twiddles 1/coord(domain.at(bitrev(2i))) for the coset `which`
+// (half_coset -> y, half_odds -> x), cached per (device, which, log_n).
+int get_fold_twiddles(int which, uint32_t log_n, const uint32_t** out, cudaStream_t st);
+int release_twiddles();
+
+int launch_batch_inverse(const uint32_t* in, uint32_t* out, uint64_t n, cudaStream_t st);
+int launch_coset_points(cpt initial, cpt step, uint32_t* ox, uint32_t* oy, uint64_t n, cudaStream_t st);
+
+}  // namespace vs
