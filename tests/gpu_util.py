@@ -28,13 +28,30 @@ def host(t: torch.Tensor) -> np.ndarray:
     return t.cpu().numpy().view(np.uint32)
 
 
+# Every tensor whose raw pointer is handed to the library stays referenced here
+# until the test has synchronised (tests/conftest.py clears it after each test):
+# a temporary freed while a launch is queued would be recycled by torch's caching
+# allocator and the kernel would read someone else's data.
+KEEP: list = []
+
+
 def ptr(t: torch.Tensor) -> int:
+    KEEP.append(t)
     return t.data_ptr()
 
 
 def ptr_array(ts) -> torch.Tensor:
-    """Device array of device pointers (uint32_t**)."""
-    return torch.tensor([t.data_ptr() for t in ts], dtype=torch.int64, device="cuda")
+    """Device array of device pointers (uint32_t**); keeps the columns alive too."""
+    ts = list(ts)
+    KEEP.extend(ts)
+    arr = torch.tensor([t.data_ptr() for t in ts], dtype=torch.int64, device="cuda")
+    KEEP.append(arr)
+    return arr
+
+
+def release() -> None:
+    torch.cuda.synchronize()
+    KEEP.clear()
 
 
 def u32_host(vals) -> C.Array:
