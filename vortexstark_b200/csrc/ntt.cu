@@ -32,20 +32,6 @@ namespace vs {
 
 __device__ __forceinline__ uint32_t swz(uint32_t a) { return a ^ ((a >> 5) & 31u); }
 
-// Twiddle for layer j at group index h.
-__device__ __forceinline__ uint32_t twiddle(const NttTw& tw, uint32_t j, uint32_t h) {
-  if (j == 0 && tw.stwo) {  // circle_ntt_stwo.cu:202-248: [y, -y, -x, x] from pairs of line layer 0
-    uint32_t x = __ldg(tw.flat + 2 * (h >> 2)), y = __ldg(tw.flat + 2 * (h >> 2) + 1);
-    switch (h & 3) {
-      case 0: return y;
-      case 1: return neg(y);
-      case 2: return neg(x);
-      default: return x;
-    }
-  }
-  return __ldg(tw.layer[j] + h);
-}
-
 template <bool FWD>
 __device__ __forceinline__ void bfly(uint32_t& v0, uint32_t& v1, uint32_t t) {
   if (FWD) {
@@ -59,109 +45,153 @@ __device__ __forceinline__ void bfly(uint32_t& v0, uint32_t& v1, uint32_t t) {
   }
 }
 
-// Tile geometry for one pass.
-struct Geo {
-  uint32_t T;       // log2 tile elements
-  uint32_t c;       // low bits kept contiguous
-  uint32_t a, b;    // layer range
-  uint32_t hi;      // tile's index bits above b
-  uint32_t gbase;   // hi << (b+1) | lo_chunk << c
-  __device__ __forceinline__ uint32_t gidx(uint32_t e) const {
-    return gbase | ((e >> c) << a) | (e & ((1u << c) - 1));
-  }
+// Tile of a pass: M layers over tile bits [C, C+M); the low C index bits stay
+// contiguous for coalescing. T = M + C, 2^(T-5) threads, 32 elements each.
+// Register rounds cover tile bits [C + 5r, C + 5r + R(r)).
+template <int M, int C>
+struct Tile {
+  static constexpr int T = M + C, NT = 1 << (T - 5), SIZE = 1 << T, NR = (M + 4) / 5;
+  static constexpr int P0(int r) { return C + 5 * r; }
+  static constexpr int R(int r) { return 5 * (r + 1) <= M ? 5 : M - 5 * r; }
 };
 
-// Element address k (R bits) of subgroup `o` inserted at bit p0.
-__device__ __forceinline__ uint32_t ins(uint32_t o, uint32_t k, uint32_t p0, uint32_t R) {
-  return ((o >> p0) << (p0 + R)) | (k << p0) | (o & ((1u << p0) - 1));
+// Runtime part of a tile's placement in the transform.
+struct TileGeo {
+  uint32_t a;      // first layer of the pass
+  uint32_t hi;     // index bits above the pass (the twiddle group prefix)
+  uint32_t gbase;  // hi << (b+1) | lo_chunk << C
+};
+
+template <int M, int C>
+__device__ __forceinline__ TileGeo tile_geo(uint32_t a, uint32_t tile) {
+  constexpr int T = M + C;
+  TileGeo g;
+  g.a = a;
+  const uint32_t lo_bits = a - C;
+  g.hi = tile >> lo_bits;
+  const uint32_t b1 = a + M;  // b + 1
+  g.gbase = (b1 >= 32 ? 0u : (g.hi << b1)) | ((tile & ((1u << lo_bits) - 1)) << C);
+  (void)T;
+  return g;
+}
+// Global index of tile element e (requires C == 0 -> a == 0 or C >= 2 for 16-byte runs).
+template <int M, int C>
+__device__ __forceinline__ uint32_t gidx(const TileGeo& g, uint32_t e) {
+  return g.gbase | ((e >> C) << g.a) | (e & ((1u << C) - 1));
 }
 
-// Butterflies of one register round: R layers at tile bits [p0, p0+R).
-// v holds SUB = 2^(5-R) subgroups of 2^R elements.
-template <int R, bool FWD>
-__device__ __forceinline__ void round_regs(uint32_t (&v)[32], const Geo& g, uint32_t p0, const NttTw& tw) {
-  constexpr int SUB = 1 << (5 - R), K = 1 << R;
-  const uint32_t nthr = 1u << (g.T - 5);
+// Coalesced 128-bit tile transfers between global memory and the swizzled tile.
+template <int M, int C>
+__device__ __forceinline__ void tile_load(uint32_t* sm, const uint32_t* __restrict__ src, const TileGeo& g,
+                                          uint32_t mask) {
+  using S = Tile<M, C>;
+#pragma unroll
+  for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
+    const uint32_t e = 4 * (threadIdx.x + i * S::NT);
+    const uint4 w = *reinterpret_cast<const uint4*>(src + (gidx<M, C>(g, e) & mask));
+    sm[swz(e)] = w.x;
+    sm[swz(e + 1)] = w.y;
+    sm[swz(e + 2)] = w.z;
+    sm[swz(e + 3)] = w.w;
+  }
+}
+template <int M, int C>
+__device__ __forceinline__ void tile_store(const uint32_t* sm, uint32_t* __restrict__ dst, const TileGeo& g) {
+  using S = Tile<M, C>;
+#pragma unroll
+  for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
+    const uint32_t e = 4 * (threadIdx.x + i * S::NT);
+    *reinterpret_cast<uint4*>(dst + gidx<M, C>(g, e)) = make_uint4(sm[swz(e)], sm[swz(e + 1)], sm[swz(e + 2)], sm[swz(e + 3)]);
+  }
+}
+
+// Address of element k (R bits) of subgroup o, inserted at tile bit P0.
+template <int P0, int R>
+__device__ __forceinline__ uint32_t ins(uint32_t o, uint32_t k) {
+  return ((o >> P0) << (P0 + R)) | (k << P0) | (o & ((1u << P0) - 1));
+}
+
+template <int M, int C, int r>
+__device__ __forceinline__ void rload(uint32_t (&v)[32], const uint32_t* sm) {
+  using S = Tile<M, C>;
+  constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (5 - R);
+#pragma unroll
+  for (int s = 0; s < SUB; s++)
+#pragma unroll
+    for (int k = 0; k < K; k++) v[s * K + k] = sm[swz(ins<P0, R>(threadIdx.x + s * S::NT, k))];
+}
+template <int M, int C, int r>
+__device__ __forceinline__ void rstore(const uint32_t (&v)[32], uint32_t* sm) {
+  using S = Tile<M, C>;
+  constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (5 - R);
+#pragma unroll
+  for (int s = 0; s < SUB; s++)
+#pragma unroll
+    for (int k = 0; k < K; k++) sm[swz(ins<P0, R>(threadIdx.x + s * S::NT, k))] = v[s * K + k];
+}
+
+// Butterflies of round r (R layers, no barrier). All of the round's twiddles are
+// fetched into registers first so their loads overlap instead of stalling each
+// butterfly. Layer at tile bit p = P0 + q is global layer j = a + p - C; its
+// group index is h = hi * 2^(T-1-p) + (address >> (p+1)).
+template <bool FWD, int M, int C, int r>
+__device__ __forceinline__ void rbfly(uint32_t (&v)[32], const TileGeo& g, const NttTw& tw) {
+  using S = Tile<M, C>;
+  constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (5 - R), T = S::T;
 #pragma unroll
   for (int s = 0; s < SUB; s++) {
-    const uint32_t o = threadIdx.x + s * nthr;
-    const uint32_t base = ins(o, 0, p0, R);
+    const uint32_t base = ins<P0, R>(threadIdx.x + s * S::NT, 0);
+    uint32_t t[K];  // layer q's twiddles at t[K - (K >> q) + gg]
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+      const int p = P0 + q;
+      const uint32_t hb = (g.hi << (T - 1 - p)) | (base >> (p + 1));
+      bool circle_stwo = false;
+      if (C == 0 && r == 0 && q == 0) circle_stwo = tw.stwo && g.a == 0;
+      if (circle_stwo) {  // circle_ntt_stwo.cu:202-248: [y, -y, -x, x] per pair of line layer 0
+        static_assert(C != 0 || R == 5 || r != 0, "round 0 of a C = 0 tile spans five layers");
+#pragma unroll
+        for (int gg = 0; gg < (K >> 1); gg += 4) {  // hb is a multiple of 4 here
+          const uint32_t pr = 2 * ((hb >> 2) + (gg >> 2));
+          const uint32_t x = __ldg(tw.flat + pr), y = __ldg(tw.flat + pr + 1);
+          t[gg] = y;
+          t[gg + 1] = neg(y);
+          t[gg + 2] = neg(x);
+          t[gg + 3] = x;
+        }
+      } else {
+        const uint32_t* tp = tw.layer[g.a + p - C] + hb;
+#pragma unroll
+        for (int gg = 0; gg < (K >> (q + 1)); gg++) t[K - (K >> q) + gg] = __ldg(tp + gg);
+      }
+    }
 #pragma unroll
     for (int qq = 0; qq < R; qq++) {
       const int q = FWD ? R - 1 - qq : qq;
-      const uint32_t p = p0 + q;                 // tile bit of this layer
-      const uint32_t j = g.a + p - g.c;          // global layer index
-      const uint32_t hbase = (g.hi << (g.b - j)) | (base >> (p + 1));
 #pragma unroll
       for (int gg = 0; gg < (K >> (q + 1)); gg++) {
-        const uint32_t t = twiddle(tw, j, hbase | gg);
+        const uint32_t tv = t[K - (K >> q) + gg];
 #pragma unroll
         for (int l = 0; l < (1 << q); l++) {
           const int k0 = (gg << (q + 1)) | l;
-          bfly<FWD>(v[s * K + k0], v[s * K + k0 + (1 << q)], t);
+          bfly<FWD>(v[s * K + k0], v[s * K + k0 + (1 << q)], tv);
         }
       }
     }
   }
 }
 
-template <int R>
-__device__ __forceinline__ void load_round(uint32_t (&v)[32], const uint32_t* sm, const Geo& g, uint32_t p0) {
-  constexpr int SUB = 1 << (5 - R), K = 1 << R;
-  const uint32_t nthr = 1u << (g.T - 5);
+// One full round through shared memory (caller provides the barrier after).
+template <bool FWD, int M, int C, int r>
+__device__ __forceinline__ void round_sm(uint32_t* sm, const TileGeo& g, const NttTw& tw, uint32_t scale) {
+  uint32_t v[32];
+  rload<M, C, r>(v, sm);
+  rbfly<FWD, M, C, r>(v, g, tw);
+  if (scale) {
 #pragma unroll
-  for (int s = 0; s < SUB; s++) {
-    const uint32_t o = threadIdx.x + s * nthr;
-#pragma unroll
-    for (int k = 0; k < K; k++) v[s * K + k] = sm[swz(ins(o, k, p0, R))];
+    for (int k = 0; k < 32; k++) v[k] = mul(v[k], scale);
   }
-}
-template <int R>
-__device__ __forceinline__ void store_round(const uint32_t (&v)[32], uint32_t* sm, const Geo& g, uint32_t p0) {
-  constexpr int SUB = 1 << (5 - R), K = 1 << R;
-  const uint32_t nthr = 1u << (g.T - 5);
-#pragma unroll
-  for (int s = 0; s < SUB; s++) {
-    const uint32_t o = threadIdx.x + s * nthr;
-#pragma unroll
-    for (int k = 0; k < K; k++) sm[swz(ins(o, k, p0, R))] = v[s * K + k];
-  }
-}
-
-template <bool FWD>
-__device__ __forceinline__ void round_any(uint32_t (&v)[32], const Geo& g, uint32_t p0, uint32_t R, const NttTw& tw) {
-  switch (R) {
-    case 1: round_regs<1, FWD>(v, g, p0, tw); break;
-    case 2: round_regs<2, FWD>(v, g, p0, tw); break;
-    case 3: round_regs<3, FWD>(v, g, p0, tw); break;
-    case 4: round_regs<4, FWD>(v, g, p0, tw); break;
-    default: round_regs<5, FWD>(v, g, p0, tw); break;
-  }
-}
-__device__ __forceinline__ void load_any(uint32_t (&v)[32], const uint32_t* sm, const Geo& g, uint32_t p0, uint32_t R) {
-  switch (R) {
-    case 1: load_round<1>(v, sm, g, p0); break;
-    case 2: load_round<2>(v, sm, g, p0); break;
-    case 3: load_round<3>(v, sm, g, p0); break;
-    case 4: load_round<4>(v, sm, g, p0); break;
-    default: load_round<5>(v, sm, g, p0); break;
-  }
-}
-__device__ __forceinline__ void store_any(const uint32_t (&v)[32], uint32_t* sm, const Geo& g, uint32_t p0, uint32_t R) {
-  switch (R) {
-    case 1: store_round<1>(v, sm, g, p0); break;
-    case 2: store_round<2>(v, sm, g, p0); break;
-    case 3: store_round<3>(v, sm, g, p0); break;
-    case 4: store_round<4>(v, sm, g, p0); break;
-    default: store_round<5>(v, sm, g, p0); break;
-  }
-}
-
-// Rounds: full five-layer rounds from tile bit c upward, the remainder (< 5) on top.
-__device__ __forceinline__ uint32_t n_rounds(uint32_t m) { return (m + 4) / 5; }
-__device__ __forceinline__ void round_span(uint32_t m, uint32_t c, uint32_t r, uint32_t& p0, uint32_t& R) {
-  p0 = c + 5 * r;
-  R = (5 * (r + 1) <= m) ? 5 : m - 5 * r;
+  rstore<M, C, r>(v, sm);
 }
 
 __device__ __forceinline__ const uint32_t* col_src(const NttPass& p) {
@@ -171,104 +201,129 @@ __device__ __forceinline__ uint32_t* col_dst(const NttPass& p) {
   return p.dst_cols ? p.dst_cols[blockIdx.y] : p.dst + (uint64_t)blockIdx.y * p.dst_stride;
 }
 
-__device__ __forceinline__ Geo make_geo(const NttPass& p, uint32_t tile) {
-  Geo g;
-  g.a = p.a;
-  g.b = p.b;
-  g.c = p.c;
-  g.T = p.b - p.a + 1 + p.c;
-  const uint32_t lo_bits = p.a - p.c;
-  const uint32_t lo_chunk = tile & ((1u << lo_bits) - 1);
-  g.hi = tile >> lo_bits;
-  g.gbase = (g.b + 1 >= 32 ? 0u : (g.hi << (g.b + 1))) | (lo_chunk << p.c);
-  return g;
-}
-
-template <bool FWD>
-__global__ void __launch_bounds__(512) ntt_pass_kernel(NttPass p) {
-  extern __shared__ uint32_t sm[];
-  const Geo g = make_geo(p, blockIdx.x);
-  const uint32_t* src = col_src(p);
-  uint32_t* dst = col_dst(p);
-  const uint32_t size = 1u << g.T, m = g.b - g.a + 1;
-  for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) sm[swz(e)] = src[g.gidx(e) & p.src_mask];
+// One pass: load tile, NR register rounds (forward: top round first), store tile.
+// The inverse scale is folded into the last round of the last inverse pass.
+template <bool FWD, int M, int C>
+__global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_pass_kernel(NttPass p) {
+  using S = Tile<M, C>;
+  __shared__ uint32_t sm[S::SIZE];
+  const TileGeo g = tile_geo<M, C>(p.a, blockIdx.x);
+  tile_load<M, C>(sm, col_src(p), g, p.src_mask);
   __syncthreads();
-  uint32_t v[32];
-  const uint32_t nr = n_rounds(m);
-  for (uint32_t rr = 0; rr < nr; rr++) {
-    const uint32_t r = FWD ? nr - 1 - rr : rr;
-    uint32_t p0, R;
-    round_span(m, g.c, r, p0, R);
-    load_any(v, sm, g, p0, R);
-    round_any<FWD>(v, g, p0, R, p.tw);
-    if (!FWD && rr == nr - 1 && p.scale) {
 #pragma unroll
-      for (int k = 0; k < 32; k++) v[k] = mul(v[k], p.scale);
+  for (int rr = 0; rr < S::NR; rr++) {
+    const uint32_t sc = (!FWD && rr == S::NR - 1) ? p.scale : 0u;
+    switch (FWD ? S::NR - 1 - rr : rr) {
+      case 0: round_sm<FWD, M, C, 0>(sm, g, p.tw, sc); break;
+      case 1: round_sm<FWD, M, C, (S::NR > 1 ? 1 : 0)>(sm, g, p.tw, sc); break;
+      default: round_sm<FWD, M, C, (S::NR > 2 ? 2 : 0)>(sm, g, p.tw, sc); break;
     }
-    store_any(v, sm, g, p0, R);  // each element is loaded and stored by the same thread within a round
     __syncthreads();
   }
-  for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) dst[g.gidx(e)] = sm[swz(e)];
+  tile_store<M, C>(sm, col_dst(p), g);
 }
 
-// Fused LDE top pass. Inverse layers [a, l-1] of the trace-domain tile (with the
-// 1/n scale), then for each blowup block q the forward layers [a, l-1] of the
-// evaluation domain on a copy of the coefficients, written to dst block q.
-// `inv` describes the trace-domain pass (src = partially interpolated trace or
-// raw input), `fwd` the evaluation-domain pass (dst, log_n = l + B). Block q's
-// tile has hi = q. If coeff_out != nullptr the coefficients are also stored.
-__global__ void __launch_bounds__(512) ntt_lde_top_kernel(NttPass inv, NttPass fwd, uint32_t B, uint32_t* coeff_out,
-                                                         uint64_t coeff_stride) {
-  extern __shared__ uint32_t sm[];
-  const Geo gi = make_geo(inv, blockIdx.x);
-  const uint32_t* src = col_src(inv);
+template <bool FWD, int M, int C>
+__device__ __forceinline__ void rounds_below_top(uint32_t* sm, const TileGeo& g, const NttTw& tw) {
+  // forward: rounds NR-2 .. 0 ; inverse: rounds 0 .. NR-2 (the top round is handled by the caller)
+  using S = Tile<M, C>;
+#pragma unroll
+  for (int rr = 0; rr + 1 < S::NR; rr++) {
+    const int r = FWD ? S::NR - 2 - rr : rr;
+    if (r == 0) round_sm<FWD, M, C, 0>(sm, g, tw, 0);
+    else round_sm<FWD, M, C, (S::NR > 2 ? 1 : 0)>(sm, g, tw, 0);
+    __syncthreads();
+  }
+}
+
+// Fused LDE top pass: inverse layers [a, l-1] of the trace tile with the 1/n
+// scale; the coefficients are parked in a second shared tile, and for each
+// blowup block q the forward layers [a, l-1] of the evaluation domain (tile
+// prefix hi = q) run on them and the result is written to dst block q.
+template <int M, int C>
+__global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_lde_top_kernel(NttPass inv, NttPass fwd, uint32_t B,
+                                                                      uint32_t* coeff_out, uint64_t coeff_stride) {
+  using S = Tile<M, C>;
+  constexpr int TOP = S::NR - 1;
+  extern __shared__ uint32_t lde_sm[];
+  uint32_t* sm = lde_sm;              // working tile
+  uint32_t* cf = lde_sm + S::SIZE;    // coefficients
+  const TileGeo gi = tile_geo<M, C>(inv.a, blockIdx.x);
+  tile_load<M, C>(sm, col_src(inv), gi, inv.src_mask);
+  __syncthreads();
+  rounds_below_top<false, M, C>(sm, gi, inv.tw);
+  {
+    uint32_t v[32];
+    rload<M, C, TOP>(v, sm);
+    rbfly<false, M, C, TOP>(v, gi, inv.tw);
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = mul(v[k], inv.scale);
+    rstore<M, C, TOP>(v, cf);
+  }
+  __syncthreads();
+  if (coeff_out) tile_store<M, C>(cf, coeff_out + (uint64_t)blockIdx.y * coeff_stride, gi);
   uint32_t* dst = col_dst(fwd);
-  const uint32_t size = 1u << gi.T, m = gi.b - gi.a + 1;
-  for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) sm[swz(e)] = src[gi.gidx(e) & inv.src_mask];
-  __syncthreads();
-  uint32_t v[32], coef[32];
-  const uint32_t nr = n_rounds(m);
-  uint32_t p0t, Rt;
-  round_span(m, gi.c, nr - 1, p0t, Rt);
-  for (uint32_t r = 0; r < nr; r++) {
-    uint32_t p0, R;
-    round_span(m, gi.c, r, p0, R);
-    load_any(v, sm, gi, p0, R);
-    round_any<false>(v, gi, p0, R, inv.tw);
-    if (r + 1 < nr) {
-      store_any(v, sm, gi, p0, R);
-      __syncthreads();
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < 32; k++) coef[k] = mul(v[k], inv.scale);
-  if (coeff_out) {
-    __syncthreads();
-    store_any(coef, sm, gi, p0t, Rt);
-    __syncthreads();
-    uint32_t* co = coeff_out + (uint64_t)blockIdx.y * coeff_stride;
-    for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) co[gi.gidx(e)] = sm[swz(e)];
-  }
   for (uint32_t q = 0; q < (1u << B); q++) {
-    Geo gf = gi;
+    TileGeo gf = gi;
     gf.hi = q;
-    gf.gbase = (q << (gi.b + 1)) | (gi.gbase & ((1u << (gi.b + 1)) - 1));
-#pragma unroll
-    for (int k = 0; k < 32; k++) v[k] = coef[k];
-    round_any<true>(v, gf, p0t, Rt, fwd.tw);
+    gf.gbase = (q << (gi.a + M)) | gi.gbase;
+    uint32_t v[32];
+    rload<M, C, TOP>(v, cf);
+    rbfly<true, M, C, TOP>(v, gf, fwd.tw);
+    rstore<M, C, TOP>(v, sm);  // the previous block's tile_store finished before the loop-end barrier
     __syncthreads();
-    store_any(v, sm, gf, p0t, Rt);
+    rounds_below_top<true, M, C>(sm, gf, fwd.tw);
+    tile_store<M, C>(sm, dst, gf);
     __syncthreads();
-    for (int r = (int)nr - 2; r >= 0; r--) {
-      uint32_t p0, R;
-      round_span(m, gi.c, r, p0, R);
-      load_any(v, sm, gf, p0, R);
-      round_any<true>(v, gf, p0, R, fwd.tw);
-      store_any(v, sm, gf, p0, R);
-      __syncthreads();
-    }
-    for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) dst[gf.gidx(e)] = sm[swz(e)];
   }
+}
+
+// Launch tables: single / lower passes use C = 0 (T = M, 5 <= M <= 13); upper
+// passes use T = 13 (C = 13 - M, 1 <= M <= 11).
+using PassFn = void (*)(NttPass);
+using TopFn = void (*)(NttPass, NttPass, uint32_t, uint32_t*, uint64_t);
+template <bool FWD, int M> PassFn pass_lo() { return ntt_pass_kernel<FWD, M, 0>; }
+template <bool FWD, int M> PassFn pass_hi() { return ntt_pass_kernel<FWD, M, 13 - M>; }
+template <int M> TopFn top_lo() { return ntt_lde_top_kernel<M, 0>; }
+template <int M> TopFn top_hi() { return ntt_lde_top_kernel<M, 13 - M>; }
+
+static PassFn pass_fn(bool fwd, uint32_t M, uint32_t C) {
+#define VS_LO(m) case m: return fwd ? pass_lo<true, m>() : pass_lo<false, m>();
+#define VS_HI(m) case m: return fwd ? pass_hi<true, m>() : pass_hi<false, m>();
+  if (C == 0) {
+    switch (M) { VS_LO(5) VS_LO(6) VS_LO(7) VS_LO(8) VS_LO(9) VS_LO(10) VS_LO(11) VS_LO(12) VS_LO(13) default: break; }
+  } else if (M + C == 13) {
+    switch (M) { VS_HI(1) VS_HI(2) VS_HI(3) VS_HI(4) VS_HI(5) VS_HI(6) VS_HI(7) VS_HI(8) VS_HI(9) VS_HI(10) VS_HI(11) default: break; }
+  }
+#undef VS_LO
+#undef VS_HI
+  return nullptr;
+}
+static TopFn top_fn(uint32_t M, uint32_t C) {
+#define VS_LO(m) case m: return top_lo<m>();
+#define VS_HI(m) case m: return top_hi<m>();
+  if (C == 0) {
+    switch (M) { VS_LO(5) VS_LO(6) VS_LO(7) VS_LO(8) VS_LO(9) VS_LO(10) VS_LO(11) VS_LO(12) VS_LO(13) default: break; }
+  } else if (M + C == 13) {
+    switch (M) { VS_HI(1) VS_HI(2) VS_HI(3) VS_HI(4) VS_HI(5) VS_HI(6) VS_HI(7) VS_HI(8) VS_HI(9) VS_HI(10) VS_HI(11) default: break; }
+  }
+#undef VS_LO
+#undef VS_HI
+  return nullptr;
+}
+
+// Twiddle of layer j, group h (scalar path for single layers and tiny transforms).
+__device__ __forceinline__ uint32_t twiddle(const NttTw& tw, uint32_t j, uint32_t h) {
+  if (j == 0 && tw.stwo) {
+    uint32_t x = __ldg(tw.flat + 2 * (h >> 2)), y = __ldg(tw.flat + 2 * (h >> 2) + 1);
+    switch (h & 3) {
+      case 0: return y;
+      case 1: return neg(y);
+      case 2: return neg(x);
+      default: return x;
+    }
+  }
+  return __ldg(tw.layer[j] + h);
 }
 
 // Single layer (cuda_circle_ntt_layer, and transforms below 32 points).
@@ -315,23 +370,12 @@ uint32_t inv_n_scale(uint32_t log_n) {
   return e == 0 ? 1u : (1u << e);
 }
 
-static int set_smem(const void* fn, uint32_t bytes) {
-  if (bytes > 48 * 1024) VS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  return VS_OK;
-}
-
 static int launch_pass(NttPass p, bool fwd, uint32_t n_cols, cudaStream_t st) {
-  const uint32_t T = p.b - p.a + 1 + p.c;
+  const uint32_t M = p.b - p.a + 1, T = M + p.c;
+  PassFn fn = pass_fn(fwd, M, p.c);
+  if (!fn) return set_error(VS_ERR_INVALID, "ntt: no kernel for pass shape M=%u C=%u", M, p.c);
   const uint32_t tiles = 1u << (p.log_n - T);
-  const uint32_t threads = 1u << (T - 5), smem = 4u << T;
-  dim3 grid(tiles, n_cols);
-  if (fwd) {
-    VS_TRY(set_smem((const void*)ntt_pass_kernel<true>, smem));
-    ntt_pass_kernel<true><<<grid, threads, smem, st>>>(p);
-  } else {
-    VS_TRY(set_smem((const void*)ntt_pass_kernel<false>, smem));
-    ntt_pass_kernel<false><<<grid, threads, smem, st>>>(p);
-  }
+  fn<<<dim3(tiles, n_cols), 1u << (T - 5), 0, st>>>(p);
   VS_LAUNCHED("ntt_pass_kernel");
   return VS_OK;
 }
@@ -423,10 +467,12 @@ int ntt_lde(const NttColumns& io, uint32_t l, uint32_t B, const NttTw& tw_inv, c
     pf.log_n = l + B;
     pf.dst = io.dst;
     pf.dst_stride = io.dst_stride;
-    const uint32_t T = r.b - r.a + 1 + r.c;
-    const uint32_t tiles = 1u << (l - T), threads = 1u << (T - 5), smem = 4u << T;
-    VS_TRY(set_smem((const void*)ntt_lde_top_kernel, smem));
-    ntt_lde_top_kernel<<<dim3(tiles, io.n_cols), threads, smem, st>>>(pi, pf, B, coeff_out, coeff_stride);
+    const uint32_t M = r.b - r.a + 1, T = M + r.c;
+    TopFn fn = top_fn(M, r.c);
+    if (!fn) return set_error(VS_ERR_INVALID, "ntt: no LDE kernel for shape M=%u C=%u", M, r.c);
+    const uint32_t smem = 8u << T;  // working tile + coefficient tile
+    VS_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    fn<<<dim3(1u << (l - T), io.n_cols), 1u << (T - 5), smem, st>>>(pi, pf, B, coeff_out, coeff_stride);
     VS_LAUNCHED("ntt_lde_top_kernel");
   }
   // 3. forward passes below the top one over the whole evaluation domain
