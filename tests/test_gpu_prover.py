@@ -40,7 +40,7 @@ def test_prove_inputs(L, a, b):
     assert gpu_prove(L, a, b, 6) == O.prove(a, b, 6)
 
 
-def test_prove_config0_size(L):
+def test_prove_log16_seeded(L):
     """log_n = 16 (65,536 rows), a1 seeded: the plain single-proof workload."""
     a1 = int(O.seeded_m31(0x56530000, 1)[0])
     p = gpu_prove(L, 1, a1, 16)
