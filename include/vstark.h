@@ -193,6 +193,17 @@ int vs_lde_native(const uint32_t* d_src, uint64_t src_stride, uint32_t* d_dst, u
  * sizes). Column c at d_cols + c*stride. root written to d_root (device, 8 words). */
 int vs_merkle_root_rowpacked(const uint32_t* d_cols, uint64_t stride, uint32_t n_cols, uint32_t log_leaves,
                              uint32_t* d_root, vs_stream_t stream);
+/* Same root as vs_merkle_root_rowpacked, but allocates no device memory: its
+ * intermediate subtree roots live in a fixed 2.1 MB array inside the library
+ * (held by every GPU that loads it, until exit), for callers that cannot allocate
+ * at that point (a server whose HBM is fully reserved by its admission budget, a
+ * framework whose allocator owns device memory, a step that must not risk an
+ * allocation failure or sync). No counterpart in the reference. Accepts at most
+ * 2^26 leaves (VS_ERR_INVALID beyond). The first call on a device looks up the
+ * array's device address; make it before any stream capture. All calls share the
+ * array: calls whose work overlaps on the GPU race. */
+int vs_merkle_root_rowpacked_noalloc(const uint32_t* d_cols, uint64_t stride, uint32_t n_cols, uint32_t log_leaves,
+                                     uint32_t* d_root, vs_stream_t stream);
 /* Merkle root with the reference's <=16-column leaf (blake2s.cu leaf semantics). */
 int vs_merkle_root_capped(const uint32_t* d_cols, uint64_t stride, uint32_t n_cols, uint32_t log_leaves,
                           uint32_t* d_root, vs_stream_t stream);
