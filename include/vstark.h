@@ -236,6 +236,48 @@ int vs_prove_fib(uint32_t a, uint32_t b, uint32_t log_n, uint8_t* h_out, uint64_
  * accepted, VS_ERR_INVALID otherwise with the reason in err (host). */
 int vs_verify_fib(const uint8_t* h_proof, uint64_t len, char* err, uint64_t err_cap);
 
+/* Graph-captured Fibonacci prover for one trace size (2^log_n rows): the whole
+ * proof (trace, LDE, commitments, device-side Fiat-Shamir channel, FRI, queries,
+ * decommitment) is one CUDA graph launch on the prover's own stream; same KRAK v1
+ * bytes as vs_prove_fib. One proof in flight per handle. */
+int vs_prover_create(uint32_t log_n, void** prover);
+int vs_prover_prove(void* prover, uint32_t a, uint32_t b, uint8_t* h_out, uint64_t cap, uint64_t* out_len);
+int vs_prover_destroy(void* prover);
+
+/* Batched / served execution. An engine owns n_slots workers (host thread +
+ * CUDA stream + cached per-shape workspaces). Submitted jobs queue in FIFO order;
+ * a free slot starts the head job when the working sets of the running jobs plus
+ * the head job fit hbm_budget_bytes (0 = unlimited; a job larger than the budget
+ * runs alone). Results: a KRAK proof for VS_JOB_FIB, the 32-byte row-packed root
+ * of the seeded columns' x4 stwo LDE for VS_JOB_COMMIT. Times are seconds since
+ * engine creation. */
+enum { VS_JOB_FIB = 0, VS_JOB_COMMIT = 1 };
+typedef struct {
+  uint32_t kind;   /* VS_JOB_FIB or VS_JOB_COMMIT */
+  uint32_t log_n;  /* log2 of the trace rows */
+  uint32_t a, b;   /* Fibonacci public inputs (t0, t1) */
+  uint32_t n_cols; /* commitment: number of columns */
+  uint32_t pad;
+  uint64_t seed;   /* commitment: seed of the uniform-M31 columns (vs_fill_uniform_m31) */
+} vs_job;
+typedef struct {
+  int status;
+  uint32_t pad;
+  uint64_t out_len;
+  double t_submit, t_start, t_end;
+} vs_job_result;
+int vs_engine_create(uint32_t n_slots, uint64_t hbm_budget_bytes, void** engine);
+int vs_engine_destroy(void* engine);
+/* Builds the workspace for this job shape in every slot (outside any timing). */
+int vs_engine_prepare(void* engine, const vs_job* shape);
+int vs_engine_submit(void* engine, const vs_job* job, uint64_t* ticket);
+/* Blocks until the job is done. With h_out == NULL only the result record is
+ * filled (the bytes stay available); otherwise the bytes are copied and the
+ * ticket is retired. */
+int vs_engine_wait(void* engine, uint64_t ticket, vs_job_result* result, uint8_t* h_out, uint64_t cap);
+int vs_engine_drain(void* engine);
+double vs_engine_now(void* engine);
+
 /* Release cached twiddles and scratch of the current device. */
 int vs_release_caches(void);
 

@@ -36,6 +36,7 @@ _CTYPES = {
     "vs_stream_t": C.c_void_p,
     "const char*": C.c_char_p,
     "char*": C.c_char_p,
+    "double": C.c_double,
 }
 
 

@@ -14,9 +14,7 @@ int launch_hash_nodes(const uint32_t* children, uint32_t* parents, uint64_t n_pa
 
 template <class Leaf>
 int merkle_tile_roots(const Leaf& leaf, uint64_t n_leaves, uint32_t TL, uint32_t* roots, cudaStream_t st) {
-  const unsigned smem = merkle_smem_bytes(TL);
-  if (smem > 48 * 1024)
-    VS_CUDA(cudaFuncSetAttribute(merkle_subtree_kernel<Leaf>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const unsigned smem = merkle_smem_bytes(TL);  // at most 48 KiB (TL <= 10): no opt-in needed
   const uint64_t tiles = (n_leaves + (1ull << TL) - 1) >> TL;
   merkle_subtree_kernel<Leaf><<<(unsigned)tiles, MK_THREADS, smem, st>>>(leaf, TL, n_leaves, roots);
   VS_LAUNCHED("merkle_subtree_kernel");

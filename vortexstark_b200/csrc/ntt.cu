@@ -21,6 +21,8 @@
 // forward top pass for each of the 2^B blowup blocks (the top B forward layers
 // of a zero-padded input only replicate the coefficients), so neither the
 // coefficients nor the zero padding touch HBM.
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "ntt.h"
@@ -370,6 +372,19 @@ uint32_t inv_n_scale(uint32_t log_n) {
   return e == 0 ? 1u : (1u << e);
 }
 
+// Opts a kernel into more than 48 KiB of dynamic shared memory, once per
+// function (so repeated and graph-captured launches make no attribute calls).
+static int allow_smem(const void* fn, uint32_t bytes) {
+  static std::mutex mu;
+  static std::map<const void*, uint32_t> done;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = done.find(fn);
+  if (it != done.end() && it->second >= bytes) return VS_OK;
+  VS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  done[fn] = bytes;
+  return VS_OK;
+}
+
 static int launch_pass(NttPass p, bool fwd, uint32_t n_cols, cudaStream_t st) {
   const uint32_t M = p.b - p.a + 1, T = M + p.c;
   PassFn fn = pass_fn(fwd, M, p.c);
@@ -471,7 +486,7 @@ int ntt_lde(const NttColumns& io, uint32_t l, uint32_t B, const NttTw& tw_inv, c
     TopFn fn = top_fn(M, r.c);
     if (!fn) return set_error(VS_ERR_INVALID, "ntt: no LDE kernel for shape M=%u C=%u", M, r.c);
     const uint32_t smem = 8u << T;  // working tile + coefficient tile
-    VS_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    VS_TRY(allow_smem((const void*)fn, smem));
     fn<<<dim3(1u << (l - T), io.n_cols), 1u << (T - 5), smem, st>>>(pi, pf, B, coeff_out, coeff_stride);
     VS_LAUNCHED("ntt_lde_top_kernel");
   }

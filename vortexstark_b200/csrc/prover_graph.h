@@ -1,0 +1,31 @@
+// Graph-captured Fibonacci prover (one instance = one slot for one trace size).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+namespace vs {
+
+class GraphProver {
+ public:
+  GraphProver();
+  ~GraphProver();
+  // Allocates the workspace on the current device, builds twiddles and captures the graph.
+  int init(uint32_t log_n);
+  // Starts a proof (one in flight per instance); finish() waits and serialises KRAK v1.
+  int launch(uint32_t a, uint32_t b);
+  int finish(uint32_t a, uint32_t b, std::vector<uint8_t>& out);
+  bool busy() const;
+  uint32_t log_n() const;
+  int device() const;
+  cudaStream_t stream() const;
+  uint64_t device_bytes() const;
+
+ private:
+  struct Impl;
+  std::unique_ptr<Impl> impl;
+};
+
+}  // namespace vs
