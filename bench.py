@@ -166,6 +166,52 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- proof workloads
+def proof_workloads(args):
+    """Plain (one Fibonacci proof at a time, log_n 16), batched (64 mixed jobs at
+    once vs the same list one at a time) and served (Poisson arrivals) runs over
+    the slot engine. Timing is host wall clock around completed jobs."""
+    from vortexstark_b200 import api
+    from vortexstark_b200 import workloads as W
+
+    out = {}
+    plain = W.plain_jobs(40, 16)
+    with api.Engine(1) as eng:
+        eng.prepare(plain[0])
+        W.run_list(eng, plain[:5], sequential=True)
+        span, res = W.run_list(eng, plain, sequential=True)
+        lat = [(r[3] - r[1]) * 1e3 for r in res]
+        ok, why = api.verify_fib(res[0][0])
+        out["plain"] = {"workload": "Fibonacci log_n=16 (a0=1, a1 seeded), one proof at a time",
+                        "proofs_per_s": len(plain) / span, "p50_ms": W.percentile(lat, 0.5),
+                        "p99_ms": W.percentile(lat, 0.99), "verified": ok}
+    jobs = W.batched_jobs(64)
+    n_fib = sum(1 for j in jobs if j.kind == api.FIB)
+    with api.Engine(1) as one:
+        for j in W.shapes(jobs):
+            one.prepare(api.commit_job(j.log_n, 34, 0) if j.kind == api.COMMIT else j)
+        t_one, r_one = W.run_list(one, jobs, sequential=True)
+    with api.Engine(args.slots) as eng:
+        for j in W.shapes(jobs):
+            eng.prepare(api.commit_job(j.log_n, 34, 0) if j.kind == api.COMMIT else j)
+        W.run_list(eng, jobs[:8], sequential=False)
+        t_b, r_b = W.run_list(eng, jobs, sequential=False)
+    same = all(a[0] == b[0] for a, b in zip(r_one, r_b))
+    out["batched"] = {"workload": "64 jobs, log_n U{16..22}: Fibonacci proofs or 1-34 uniform columns (commit)",
+                      "slots": args.slots, "jobs_per_s": len(jobs) / t_b, "proofs_per_s": n_fib / t_b,
+                      "one_at_a_time_jobs_per_s": len(jobs) / t_one, "speedup_vs_one_at_a_time": t_one / t_b,
+                      "results_identical_alone_vs_batched": same}
+    arrivals = W.served_arrivals(args.served_jobs)
+    with api.Engine(args.slots, 150 * 10**9) as eng:
+        for j in W.shapes([a[1] for a in arrivals]):
+            eng.prepare(api.commit_job(j.log_n, 34, 0) if j.kind == api.COMMIT else j)
+        recs = W.run_served(eng, arrivals)
+    out["served"] = dict(W.summarize_served(recs), workload="Poisson 200 jobs/s: Fibonacci 16/20/24 (0.5/0.3/0.2) "
+                         "and 34-col commits 18/20/22", slots=args.slots, hbm_budget_gb=150)
+    out["batched_vs_plain_proofs_per_s"] = out["batched"]["proofs_per_s"] / out["plain"]["proofs_per_s"]
+    return out
+
+
 # ---------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -179,6 +225,9 @@ def main():
     ap.add_argument("--cpu-log-n", type=int, default=16, help="row log of the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-proofs", action="store_true", help="skip the plain / batched / served proof runs")
+    ap.add_argument("--slots", type=int, default=8, help="concurrent slots of the batched and served engines")
+    ap.add_argument("--served-jobs", type=int, default=600)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -306,13 +355,18 @@ def main():
             "traffic": None, "phase_ms": phase,
             "phase_hbm_frac": {k: alg[k] / (phase[k] / 1e3) / 1e9 / hbm for k in phase}}
 
+    proofs = None
+    if rank == 0 and world == 1 and not args.no_proofs:
+        del lde, cols, fri_src, work
+        torch.cuda.empty_cache()
+        proofs = proof_workloads(args)
     if rank == 0:
         cpu = None if args.no_cpu else cpu_sample(args, os.cpu_count() or 1)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic (seeded SplitMix64 uniform M31)",
                 "config": config_json(args), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": clk.summary()}
+                "gpu_launches": launches, "clocks": clk.summary(), "proofs": proofs}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

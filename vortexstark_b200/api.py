@@ -80,3 +80,66 @@ def verify_fib(proof: bytes) -> tuple[bool, str]:
 
 def launch_count() -> int:
     return int(lib().vs_launch_count())
+
+
+# ---------------------------------------------------------------- batched / served proving
+class Job(C.Structure):
+    """vs_job: kind 0 = Fibonacci proof (log_n, a, b), 1 = column commitment (log_n, n_cols, seed)."""
+    _fields_ = [("kind", C.c_uint32), ("log_n", C.c_uint32), ("a", C.c_uint32), ("b", C.c_uint32),
+                ("n_cols", C.c_uint32), ("pad", C.c_uint32), ("seed", C.c_uint64)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("pad", C.c_uint32), ("out_len", C.c_uint64), ("t_submit", C.c_double),
+                ("t_start", C.c_double), ("t_end", C.c_double)]
+
+
+FIB, COMMIT = 0, 1
+
+
+def fib_job(log_n: int, a: int, b: int) -> Job:
+    return Job(FIB, log_n, a, b, 0, 0, 0)
+
+
+def commit_job(log_n: int, n_cols: int, seed: int) -> Job:
+    return Job(COMMIT, log_n, 0, 0, n_cols, 0, seed)
+
+
+class Engine:
+    """Slots of concurrent provers with FIFO admission against an HBM budget."""
+
+    def __init__(self, slots: int, hbm_budget_bytes: int = 0):
+        self.h = C.c_void_p()
+        check(lib().vs_engine_create(slots, hbm_budget_bytes, C.byref(self.h)), "vs_engine_create")
+        self._buf = (C.c_uint8 * PROOF_CAP)()
+
+    def prepare(self, job: Job) -> None:
+        check(lib().vs_engine_prepare(self.h, C.byref(job)), "vs_engine_prepare")
+
+    def submit(self, job: Job) -> int:
+        t = C.c_uint64()
+        check(lib().vs_engine_submit(self.h, C.byref(job), C.byref(t)), "vs_engine_submit")
+        return t.value
+
+    def wait(self, ticket: int):
+        """Returns (result bytes, t_submit, t_start, t_end) in engine seconds."""
+        r = JobResult()
+        check(lib().vs_engine_wait(self.h, ticket, C.byref(r), self._buf, PROOF_CAP), "vs_engine_wait")
+        return bytes(self._buf[: r.out_len]), r.t_submit, r.t_start, r.t_end
+
+    def drain(self) -> None:
+        lib().vs_engine_drain(self.h)
+
+    def now(self) -> float:
+        return lib().vs_engine_now(self.h)
+
+    def close(self) -> None:
+        if self.h:
+            lib().vs_engine_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -27,13 +27,15 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
-uint64_t shape_key(const vs_job& j) {
-  return ((uint64_t)j.kind << 48) | ((uint64_t)j.log_n << 32) | (j.kind == VS_JOB_COMMIT ? j.n_cols : 0);
-}
+// Workspaces are cached per (kind, log_n); commitment buffers hold at least
+// kCommitCols columns and grow for wider jobs.
+constexpr uint32_t kCommitCols = 34;
+uint64_t shape_key(const vs_job& j) { return ((uint64_t)j.kind << 32) | j.log_n; }
 
 struct CommitWs {
   uint32_t *cols = nullptr, *lde = nullptr, *root = nullptr, *scratch = nullptr, *h_root = nullptr;
   uint64_t bytes = 0;
+  uint32_t capacity = 0;  // columns
   ~CommitWs() {
     if (cols) cudaFree(cols);
     if (lde) cudaFree(lde);
@@ -96,15 +98,17 @@ struct Engine {
   }
   int commit_for(Slot& s, const vs_job& j, CommitWs** out) {
     auto& c = s.commits[shape_key(j)];
-    if (!c) {
+    if (!c || c->capacity < j.n_cols) {
+      c.reset();
       auto w = std::make_unique<CommitWs>();
       const uint64_t n = 1ull << j.log_n, N = n << 2;
-      VS_CUDA(cudaMalloc(&w->cols, (uint64_t)j.n_cols * n * 4));
-      VS_CUDA(cudaMalloc(&w->lde, (uint64_t)j.n_cols * N * 4));
+      w->capacity = std::max(kCommitCols, j.n_cols);
+      VS_CUDA(cudaMalloc(&w->cols, (uint64_t)w->capacity * n * 4));
+      VS_CUDA(cudaMalloc(&w->lde, (uint64_t)w->capacity * N * 4));
       VS_CUDA(cudaMalloc(&w->root, 32));
       VS_CUDA(cudaMalloc(&w->scratch, std::max<uint64_t>(merkle_scratch_words(N), 8) * 4));
       VS_CUDA(cudaMallocHost(&w->h_root, 32));
-      w->bytes = commit_bytes(j.log_n, j.n_cols);
+      w->bytes = commit_bytes(j.log_n, w->capacity);
       const TwiddleSet* t = nullptr;
       VS_TRY(get_twiddles(TW_STWO, j.log_n, &t, s.st));
       VS_TRY(get_twiddles(TW_STWO, j.log_n + 2, &t, s.st));
