@@ -168,47 +168,63 @@ def run_reference(args):
 
 # ---------------------------------------------------------------- proof workloads
 def proof_workloads(args):
-    """Plain (one Fibonacci proof at a time, log_n 16), batched (64 mixed jobs at
-    once vs the same list one at a time) and served (Poisson arrivals) runs over
-    the slot engine. Timing is host wall clock around completed jobs."""
+    """Proof throughput and latency. The plain path is the drop-in single-job
+    entry points (vs_prove_fib, vs_commit_columns) called one job at a time; the
+    engine runs the same jobs over slots of graph-captured provers. Timing is host
+    wall clock around completed jobs (results back in host memory)."""
     from vortexstark_b200 import api
     from vortexstark_b200 import workloads as W
 
-    out = {}
-    plain = W.plain_jobs(40, 16)
-    with api.Engine(1) as eng:
-        eng.prepare(plain[0])
-        W.run_list(eng, plain[:5], sequential=True)
-        span, res = W.run_list(eng, plain, sequential=True)
-        lat = [(r[3] - r[1]) * 1e3 for r in res]
-        ok, why = api.verify_fib(res[0][0])
-        out["plain"] = {"workload": "Fibonacci log_n=16 (a0=1, a1 seeded), one proof at a time",
-                        "proofs_per_s": len(plain) / span, "p50_ms": W.percentile(lat, 0.5),
-                        "p99_ms": W.percentile(lat, 0.99), "verified": ok}
-    jobs = W.batched_jobs(64)
-    n_fib = sum(1 for j in jobs if j.kind == api.FIB)
-    with api.Engine(1) as one:
+    def prep(eng, jobs):
         for j in W.shapes(jobs):
-            one.prepare(api.commit_job(j.log_n, 34, 0) if j.kind == api.COMMIT else j)
+            eng.prepare(api.commit_job(j.log_n, 34, 0) if j.kind == api.COMMIT else j)
+
+    out = {}
+    plain = W.plain_jobs(64, 16)
+    W.run_plain(plain[:4])
+    t_plain, r_plain = W.run_plain(plain)
+    lat = []
+    for j in plain[:32]:
+        t0 = time.perf_counter()
+        api.prove_fib(j.a, j.b, j.log_n)
+        lat.append((time.perf_counter() - t0) * 1e3)
+    ok, _ = api.verify_fib(r_plain[0])
+    out["plain"] = {"workload": "64 Fibonacci proofs, log_n=16, a0=1, a1 seeded; vs_prove_fib one at a time",
+                    "proofs_per_s": len(plain) / t_plain, "p50_ms": W.percentile(lat, 0.5),
+                    "p99_ms": W.percentile(lat, 0.99), "verified": ok}
+    with api.Engine(args.slots) as eng:
+        prep(eng, plain)
+        W.run_list(eng, plain[:16], sequential=False)
+        t_e, r_e = W.run_list(eng, plain, sequential=False)
+    out["batched_fib16"] = {"workload": "the same 64 proofs submitted at once to the slot engine",
+                            "slots": args.slots, "proofs_per_s": len(plain) / t_e,
+                            "vs_plain": t_plain / t_e,
+                            "identical_to_plain": all(x[0] == y for x, y in zip(r_e, r_plain))}
+
+    jobs = W.batched_jobs(64)
+    W.run_plain(W.shapes(jobs))
+    t_p, r_p = W.run_plain(jobs)
+    with api.Engine(1) as one:
+        prep(one, jobs)
         t_one, r_one = W.run_list(one, jobs, sequential=True)
     with api.Engine(args.slots) as eng:
-        for j in W.shapes(jobs):
-            eng.prepare(api.commit_job(j.log_n, 34, 0) if j.kind == api.COMMIT else j)
+        prep(eng, jobs)
         W.run_list(eng, jobs[:8], sequential=False)
         t_b, r_b = W.run_list(eng, jobs, sequential=False)
-    same = all(a[0] == b[0] for a, b in zip(r_one, r_b))
-    out["batched"] = {"workload": "64 jobs, log_n U{16..22}: Fibonacci proofs or 1-34 uniform columns (commit)",
-                      "slots": args.slots, "jobs_per_s": len(jobs) / t_b, "proofs_per_s": n_fib / t_b,
-                      "one_at_a_time_jobs_per_s": len(jobs) / t_one, "speedup_vs_one_at_a_time": t_one / t_b,
-                      "results_identical_alone_vs_batched": same}
+    n_fib = sum(1 for j in jobs if j.kind == api.FIB)
+    out["batched_mix"] = {
+        "workload": "64 jobs, log_n U{16..22}: Fibonacci proofs (a1 seeded) or 1-34 seeded uniform columns (commit)",
+        "slots": args.slots, "jobs_per_s": len(jobs) / t_b, "proofs_per_s": n_fib / t_b,
+        "plain_path_jobs_per_s": len(jobs) / t_p, "engine_one_slot_jobs_per_s": len(jobs) / t_one,
+        "vs_plain": t_p / t_b, "vs_one_slot": t_one / t_b,
+        "identical_plain_one_slot_batched": all(a == b[0] == c[0] for a, b, c in zip(r_p, r_one, r_b))}
+
     arrivals = W.served_arrivals(args.served_jobs)
     with api.Engine(args.slots, 150 * 10**9) as eng:
-        for j in W.shapes([a[1] for a in arrivals]):
-            eng.prepare(api.commit_job(j.log_n, 34, 0) if j.kind == api.COMMIT else j)
+        prep(eng, [a[1] for a in arrivals])
         recs = W.run_served(eng, arrivals)
     out["served"] = dict(W.summarize_served(recs), workload="Poisson 200 jobs/s: Fibonacci 16/20/24 (0.5/0.3/0.2) "
                          "and 34-col commits 18/20/22", slots=args.slots, hbm_budget_gb=150)
-    out["batched_vs_plain_proofs_per_s"] = out["batched"]["proofs_per_s"] / out["plain"]["proofs_per_s"]
     return out
 
 
@@ -222,7 +238,8 @@ def main():
     ap.add_argument("--cols", type=int, default=34)
     ap.add_argument("--log-n", type=int, default=24)
     ap.add_argument("--fri-log", type=int, default=26)
-    ap.add_argument("--cpu-log-n", type=int, default=16, help="row log of the CPU baseline sample")
+    ap.add_argument("--cpu-log-n", type=int, default=None,
+                    help="row log of the CPU sample (default 22 for the cpu_baseline, 20 per reference-arm step)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-proofs", action="store_true", help="skip the plain / batched / served proof runs")
@@ -230,6 +247,8 @@ def main():
     ap.add_argument("--served-jobs", type=int, default=600)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.cpu_log_n is None:
+        args.cpu_log_n = 20 if args.impl == "reference" else 22
     if args.impl == "reference":
         return run_reference(args)
 

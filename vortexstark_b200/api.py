@@ -8,6 +8,7 @@ Tensors are int32 views of u32 field words, on a CUDA device.
 from __future__ import annotations
 
 import ctypes as C
+import threading
 
 import torch
 
@@ -63,12 +64,34 @@ def fri_fold_commit(src: torch.Tensor, log_n: int, alphas, work: torch.Tensor, r
           "vs_fri_fold_commit")
 
 
+_tls = threading.local()
+
+
+def _proof_buffer():
+    """One reusable host buffer per thread for proofs coming back from the library."""
+    buf = getattr(_tls, "buf", None)
+    if buf is None:
+        buf = _tls.buf = (C.c_uint8 * PROOF_CAP)()
+    return buf
+
+
 def prove_fib(a: int, b: int, log_n: int, stream=None) -> bytes:
     """Fibonacci proof in the KRAK v1 wire format."""
-    buf = (C.c_uint8 * PROOF_CAP)()
+    buf = _proof_buffer()
     n = C.c_uint64(0)
     check(lib().vs_prove_fib(a, b, log_n, buf, PROOF_CAP, C.byref(n), _stream(stream)), "vs_prove_fib")
-    return bytes(buf[: n.value])
+    return C.string_at(buf, n.value)
+
+
+def commit_seeded(log_n: int, n_cols: int, seed: int, blowup: int = 2, stream=None) -> bytes:
+    """Root of n_cols seeded uniform-M31 columns of 2^log_n rows (stwo LDE + row-packed Merkle),
+    one call at a time through the drop-in entry points."""
+    dev = torch.device("cuda", torch.cuda.current_device())
+    cols = fill_uniform_m31(torch.empty((n_cols, 1 << log_n), dtype=torch.int32, device=dev), seed, 0, stream)
+    lde = torch.empty((n_cols, 1 << (log_n + blowup)), dtype=torch.int32, device=dev)
+    root = torch.empty(8, dtype=torch.int32, device=dev)
+    commit_columns(cols, log_n, blowup, lde, root, stream)
+    return root.cpu().numpy().tobytes()
 
 
 def verify_fib(proof: bytes) -> tuple[bool, str]:
@@ -125,7 +148,7 @@ class Engine:
         """Returns (result bytes, t_submit, t_start, t_end) in engine seconds."""
         r = JobResult()
         check(lib().vs_engine_wait(self.h, ticket, C.byref(r), self._buf, PROOF_CAP), "vs_engine_wait")
-        return bytes(self._buf[: r.out_len]), r.t_submit, r.t_start, r.t_end
+        return C.string_at(self._buf, r.out_len), r.t_submit, r.t_start, r.t_end
 
     def drain(self) -> None:
         lib().vs_engine_drain(self.h)

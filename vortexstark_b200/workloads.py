@@ -16,7 +16,7 @@ import statistics
 import threading
 import time
 
-from .api import COMMIT, FIB, Engine, commit_job, fib_job
+from .api import COMMIT, FIB, Engine, commit_job, commit_seeded, fib_job, prove_fib
 
 P = 0x7FFFFFFF
 
@@ -101,6 +101,23 @@ def run_list(engine: Engine, jobs, sequential: bool):
         tickets = [engine.submit(j) for j in jobs]
         res = [engine.wait(t) for t in tickets]
     return engine.now() - t0, res
+
+
+def run_plain(jobs):
+    """The plain single-job GPU path: each job through the drop-in entry points
+    (vs_prove_fib / vs_commit_columns), one after another. Returns (seconds, results)."""
+    import torch
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = []
+    for j in jobs:
+        if j.kind == FIB:
+            res.append(prove_fib(j.a, j.b, j.log_n))
+        else:
+            res.append(commit_seeded(j.log_n, j.n_cols, j.seed))
+    torch.cuda.synchronize()
+    return time.perf_counter() - t0, res
 
 
 def percentile(xs, q):
