@@ -11,18 +11,22 @@
 // [a, b]. A pass loads tiles of 2^(b-a+1) x 2^c elements (c low index bits kept
 // for coalescing) into shared memory, runs its layers as register rounds of up
 // to five layers (32 elements per thread, no barrier inside a round) and writes
-// the tile back once. The shared tile uses an XOR swizzle (addr ^ ((addr>>5)&31))
-// that keeps every round's access pattern bank-conflict free. A 2^24-point
-// transform is two HBM round trips instead of the reference's 24 per-layer
-// launches.
+// the tile back once. The shared tile uses a 16-byte-chunk XOR swizzle (swz)
+// that keeps every round's access pattern bank-conflict free. Pass kernels are
+// persistent (resident CTAs x SMs) and double-buffer their tiles: the next tile
+// streams in with 16-byte cp.async copies while the current one is transformed,
+// so HBM latency hides behind the integer work. A 2^24-point transform is two
+// HBM round trips instead of the reference's 24 per-layer launches.
 //
 // The LDE path fuses interpolate -> zero-pad -> evaluate: the top pass of the
 // inverse transform keeps the coefficients in registers and directly runs the
 // forward top pass for each of the 2^B blowup blocks (the top B forward layers
 // of a zero-padded input only replicate the coefficients), so neither the
 // coefficients nor the zero padding touch HBM.
+#include <algorithm>
 #include <map>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "ntt.h"
@@ -32,20 +36,49 @@
 
 namespace vs {
 
-__device__ __forceinline__ uint32_t swz(uint32_t a) { return a ^ ((a >> 5) & 31u); }
+// Shared-tile swizzle: the 16-byte chunk index (word bits 2..4) is XORed with
+// three higher word bits chosen per C, so chunks stay whole (16-byte async
+// copies and 128-bit accesses) and every register round of a tile with C low
+// bits, as well as the 16-byte tile transfers, is bank-conflict free. (C = 1 is
+// not a tile shape: its round 0 cannot be made conflict free this way.)
+template <int C>
+__device__ __forceinline__ uint32_t swz(uint32_t a) {
+  static_assert(C != 1, "no C = 1 tiles");
+  constexpr int s0 = C == 2 ? 7 : 5;
+  constexpr int s1 = (C == 2 || C == 3) ? 8 : 6;
+  constexpr int s2 = (C >= 2 && C <= 4) ? 9 : 7;
+  const uint32_t h = ((a >> s0) & 1u) | (((a >> s1) & 1u) << 1) | (((a >> s2) & 1u) << 2);
+  return a ^ (h << 2);
+}
 
+// x * t mod p from tt = 2t (< 2^32): x * tt = hi * 2^32 + lo with lo even, so
+// x * t = hi * 2^31 + lo / 2 == hi + lo / 2 (mod p), and both halves are < 2^31.
+__device__ __forceinline__ uint32_t mul_tt(uint32_t x, uint32_t tt) {
+  return canon((x * tt >> 1) + __umulhi(x, tt));
+}
+
+// Butterflies take doubled twiddles (tt = 2t).
 template <bool FWD>
-__device__ __forceinline__ void bfly(uint32_t& v0, uint32_t& v1, uint32_t t) {
+__device__ __forceinline__ void bfly(uint32_t& v0, uint32_t& v1, uint32_t tt) {
   if (FWD) {
-    uint32_t m = mul(v1, t);
+    uint32_t m = mul_tt(v1, tt);
     v1 = sub(v0, m);
     v0 = add(v0, m);
   } else {
     uint32_t s = v0;
     v0 = add(s, v1);
-    v1 = mul(sub(s, v1), t);
+    v1 = mul_tt(sub(s, v1), tt);
   }
 }
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // Tile of a pass: M layers over tile bits [C, C+M); the low C index bits stay
 // contiguous for coalescing. T = M + C, 2^(T-5) threads, 32 elements each.
@@ -90,11 +123,19 @@ __device__ __forceinline__ void tile_load(uint32_t* sm, const uint32_t* __restri
 #pragma unroll
   for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
     const uint32_t e = 4 * (threadIdx.x + i * S::NT);
-    const uint4 w = *reinterpret_cast<const uint4*>(src + (gidx<M, C>(g, e) & mask));
-    sm[swz(e)] = w.x;
-    sm[swz(e + 1)] = w.y;
-    sm[swz(e + 2)] = w.z;
-    sm[swz(e + 3)] = w.w;
+    *reinterpret_cast<uint4*>(sm + swz<C>(e)) = *reinterpret_cast<const uint4*>(src + (gidx<M, C>(g, e) & mask));
+  }
+}
+// The same load as 16-byte asynchronous copies (no registers held while in flight).
+template <int M, int C>
+__device__ __forceinline__ void tile_load_async(uint32_t* sm, const uint32_t* __restrict__ src, const TileGeo& g,
+                                                uint32_t mask) {
+  using S = Tile<M, C>;
+  const uint32_t base = smem_addr(sm);
+#pragma unroll
+  for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
+    const uint32_t e = 4 * (threadIdx.x + i * S::NT);
+    cp_async16(base + 4 * swz<C>(e), src + (gidx<M, C>(g, e) & mask));
   }
 }
 template <int M, int C>
@@ -103,7 +144,7 @@ __device__ __forceinline__ void tile_store(const uint32_t* sm, uint32_t* __restr
 #pragma unroll
   for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
     const uint32_t e = 4 * (threadIdx.x + i * S::NT);
-    *reinterpret_cast<uint4*>(dst + gidx<M, C>(g, e)) = make_uint4(sm[swz(e)], sm[swz(e + 1)], sm[swz(e + 2)], sm[swz(e + 3)]);
+    *reinterpret_cast<uint4*>(dst + gidx<M, C>(g, e)) = *reinterpret_cast<const uint4*>(sm + swz<C>(e));
   }
 }
 
@@ -113,28 +154,50 @@ __device__ __forceinline__ uint32_t ins(uint32_t o, uint32_t k) {
   return ((o >> P0) << (P0 + R)) | (k << P0) | (o & ((1u << P0) - 1));
 }
 
+// Round 0 of a C = 0 tile holds 32 consecutive words per thread: eight 128-bit
+// accesses (conflict free per quarter warp under swz<0>).
 template <int M, int C, int r>
 __device__ __forceinline__ void rload(uint32_t (&v)[32], const uint32_t* sm) {
   using S = Tile<M, C>;
   constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (5 - R);
+  if constexpr (C == 0 && r == 0) {
+    static_assert(R == 5, "C = 0 tiles start with a five-layer round");
+    const uint32_t row = threadIdx.x << 5;
 #pragma unroll
-  for (int s = 0; s < SUB; s++)
+    for (int j = 0; j < 8; j++) {
+      const uint4 w = *reinterpret_cast<const uint4*>(sm + swz<C>(row | (4 * j)));
+      v[4 * j] = w.x;
+      v[4 * j + 1] = w.y;
+      v[4 * j + 2] = w.z;
+      v[4 * j + 3] = w.w;
+    }
+  } else {
 #pragma unroll
-    for (int k = 0; k < K; k++) v[s * K + k] = sm[swz(ins<P0, R>(threadIdx.x + s * S::NT, k))];
+    for (int s = 0; s < SUB; s++)
+#pragma unroll
+      for (int k = 0; k < K; k++) v[s * K + k] = sm[swz<C>(ins<P0, R>(threadIdx.x + s * S::NT, k))];
+  }
 }
 template <int M, int C, int r>
 __device__ __forceinline__ void rstore(const uint32_t (&v)[32], uint32_t* sm) {
   using S = Tile<M, C>;
   constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (5 - R);
+  if constexpr (C == 0 && r == 0) {
+    const uint32_t row = threadIdx.x << 5;
 #pragma unroll
-  for (int s = 0; s < SUB; s++)
+    for (int j = 0; j < 8; j++)
+      *reinterpret_cast<uint4*>(sm + swz<C>(row | (4 * j))) = make_uint4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+  } else {
 #pragma unroll
-    for (int k = 0; k < K; k++) sm[swz(ins<P0, R>(threadIdx.x + s * S::NT, k))] = v[s * K + k];
+    for (int s = 0; s < SUB; s++)
+#pragma unroll
+      for (int k = 0; k < K; k++) sm[swz<C>(ins<P0, R>(threadIdx.x + s * S::NT, k))] = v[s * K + k];
+  }
 }
 
 // Butterflies of round r (R layers, no barrier). All of the round's twiddles are
-// fetched into registers first so their loads overlap instead of stalling each
-// butterfly. Layer at tile bit p = P0 + q is global layer j = a + p - C; its
+// fetched into registers first (doubled, for mul_tt) so their loads overlap
+// instead of stalling each butterfly. Layer at tile bit p = P0 + q is global layer j = a + p - C; its
 // group index is h = hi * 2^(T-1-p) + (address >> (p+1)).
 template <bool FWD, int M, int C, int r>
 __device__ __forceinline__ void rbfly(uint32_t (&v)[32], const TileGeo& g, const NttTw& tw) {
@@ -156,15 +219,15 @@ __device__ __forceinline__ void rbfly(uint32_t (&v)[32], const TileGeo& g, const
         for (int gg = 0; gg < (K >> 1); gg += 4) {  // hb is a multiple of 4 here
           const uint32_t pr = 2 * ((hb >> 2) + (gg >> 2));
           const uint32_t x = __ldg(tw.flat + pr), y = __ldg(tw.flat + pr + 1);
-          t[gg] = y;
-          t[gg + 1] = neg(y);
-          t[gg + 2] = neg(x);
-          t[gg + 3] = x;
+          t[gg] = y << 1;
+          t[gg + 1] = neg(y) << 1;
+          t[gg + 2] = neg(x) << 1;
+          t[gg + 3] = x << 1;
         }
       } else {
         const uint32_t* tp = tw.layer[g.a + p - C] + hb;
 #pragma unroll
-        for (int gg = 0; gg < (K >> (q + 1)); gg++) t[K - (K >> q) + gg] = __ldg(tp + gg);
+        for (int gg = 0; gg < (K >> (q + 1)); gg++) t[K - (K >> q) + gg] = __ldg(tp + gg) << 1;
       }
     }
 #pragma unroll
@@ -196,33 +259,52 @@ __device__ __forceinline__ void round_sm(uint32_t* sm, const TileGeo& g, const N
   rstore<M, C, r>(v, sm);
 }
 
-__device__ __forceinline__ const uint32_t* col_src(const NttPass& p) {
-  return p.src_cols ? p.src_cols[blockIdx.y] : p.src + (uint64_t)blockIdx.y * p.src_stride;
+__device__ __forceinline__ const uint32_t* col_src(const NttPass& p, uint32_t c) {
+  return p.src_cols ? p.src_cols[c] : p.src + (uint64_t)c * p.src_stride;
 }
-__device__ __forceinline__ uint32_t* col_dst(const NttPass& p) {
-  return p.dst_cols ? p.dst_cols[blockIdx.y] : p.dst + (uint64_t)blockIdx.y * p.dst_stride;
+__device__ __forceinline__ uint32_t* col_dst(const NttPass& p, uint32_t c) {
+  return p.dst_cols ? p.dst_cols[c] : p.dst + (uint64_t)c * p.dst_stride;
 }
 
-// One pass: load tile, NR register rounds (forward: top round first), store tile.
-// The inverse scale is folded into the last round of the last inverse pass.
+// One pass over work items w = column * 2^tile_bits + tile, strided by the grid.
+// Per item: NR register rounds (forward: top round first) on the shared tile,
+// then the tile is stored; the next item's tile is already in flight into the
+// other buffer. The inverse scale is folded into the last round of the last
+// inverse pass. Every thread commits one copy group per iteration (empty at the
+// end), so "wait until one group is pending" always means "this tile landed".
 template <bool FWD, int M, int C>
-__global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_pass_kernel(NttPass p) {
+__global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_pass_kernel(NttPass p, uint32_t tile_bits,
+                                                                      uint32_t total) {
   using S = Tile<M, C>;
-  __shared__ uint32_t sm[S::SIZE];
-  const TileGeo g = tile_geo<M, C>(p.a, blockIdx.x);
-  tile_load<M, C>(sm, col_src(p), g, p.src_mask);
-  __syncthreads();
-#pragma unroll
-  for (int rr = 0; rr < S::NR; rr++) {
-    const uint32_t sc = (!FWD && rr == S::NR - 1) ? p.scale : 0u;
-    switch (FWD ? S::NR - 1 - rr : rr) {
-      case 0: round_sm<FWD, M, C, 0>(sm, g, p.tw, sc); break;
-      case 1: round_sm<FWD, M, C, (S::NR > 1 ? 1 : 0)>(sm, g, p.tw, sc); break;
-      default: round_sm<FWD, M, C, (S::NR > 2 ? 2 : 0)>(sm, g, p.tw, sc); break;
-    }
+  extern __shared__ __align__(16) uint32_t pass_sm[];
+  uint32_t w = blockIdx.x;
+  if (w >= total) return;
+  const uint32_t tmask = (1u << tile_bits) - 1;
+  tile_load_async<M, C>(pass_sm, col_src(p, w >> tile_bits), tile_geo<M, C>(p.a, w & tmask), p.src_mask);
+  cp_async_commit();
+  for (uint32_t it = 0; w < total; it++, w += gridDim.x) {
+    uint32_t* sm = pass_sm + (it & 1) * S::SIZE;
+    const uint32_t nw = w + gridDim.x;
+    if (nw < total)
+      tile_load_async<M, C>(pass_sm + ((it + 1) & 1) * S::SIZE, col_src(p, nw >> tile_bits),
+                            tile_geo<M, C>(p.a, nw & tmask), p.src_mask);
+    cp_async_commit();
+    cp_async_wait1();
     __syncthreads();
+    const TileGeo g = tile_geo<M, C>(p.a, w & tmask);
+#pragma unroll
+    for (int rr = 0; rr < S::NR; rr++) {
+      const uint32_t sc = (!FWD && rr == S::NR - 1) ? p.scale : 0u;
+      switch (FWD ? S::NR - 1 - rr : rr) {
+        case 0: round_sm<FWD, M, C, 0>(sm, g, p.tw, sc); break;
+        case 1: round_sm<FWD, M, C, (S::NR > 1 ? 1 : 0)>(sm, g, p.tw, sc); break;
+        default: round_sm<FWD, M, C, (S::NR > 2 ? 2 : 0)>(sm, g, p.tw, sc); break;
+      }
+      __syncthreads();
+    }
+    tile_store<M, C>(sm, col_dst(p, w >> tile_bits), g);
+    __syncthreads();  // this buffer is refilled by the next iteration's prefetch
   }
-  tile_store<M, C>(sm, col_dst(p), g);
 }
 
 template <bool FWD, int M, int C>
@@ -251,7 +333,7 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_lde_top_kernel(NttPas
   uint32_t* sm = lde_sm;              // working tile
   uint32_t* cf = lde_sm + S::SIZE;    // coefficients
   const TileGeo gi = tile_geo<M, C>(inv.a, blockIdx.x);
-  tile_load<M, C>(sm, col_src(inv), gi, inv.src_mask);
+  tile_load<M, C>(sm, col_src(inv, blockIdx.y), gi, inv.src_mask);
   __syncthreads();
   rounds_below_top<false, M, C>(sm, gi, inv.tw);
   {
@@ -264,7 +346,7 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_lde_top_kernel(NttPas
   }
   __syncthreads();
   if (coeff_out) tile_store<M, C>(cf, coeff_out + (uint64_t)blockIdx.y * coeff_stride, gi);
-  uint32_t* dst = col_dst(fwd);
+  uint32_t* dst = col_dst(fwd, blockIdx.y);
   for (uint32_t q = 0; q < (1u << B); q++) {
     TileGeo gf = gi;
     gf.hi = q;
@@ -282,7 +364,7 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_lde_top_kernel(NttPas
 
 // Launch tables: single / lower passes use C = 0 (T = M, 5 <= M <= 13); upper
 // passes use T = 13 (C = 13 - M, 1 <= M <= 11).
-using PassFn = void (*)(NttPass);
+using PassFn = void (*)(NttPass, uint32_t, uint32_t);
 using TopFn = void (*)(NttPass, NttPass, uint32_t, uint32_t*, uint64_t);
 template <bool FWD, int M> PassFn pass_lo() { return ntt_pass_kernel<FWD, M, 0>; }
 template <bool FWD, int M> PassFn pass_hi() { return ntt_pass_kernel<FWD, M, 13 - M>; }
@@ -336,7 +418,7 @@ __global__ void ntt_layer_kernel(uint32_t* __restrict__ d, NttTw tw, uint32_t j,
   uint32_t h = tid >> j, l = tid & ((1u << j) - 1);
   uint32_t i0 = (h << (j + 1)) + l, i1 = i0 + (1u << j);
   uint32_t v0 = d[i0], v1 = d[i1];
-  bfly<FWD>(v0, v1, twiddle(tw, j, h));
+  bfly<FWD>(v0, v1, twiddle(tw, j, h) << 1);
   d[i0] = v0;
   d[i1] = v1;
 }
@@ -385,12 +467,36 @@ static int allow_smem(const void* fn, uint32_t bytes) {
   return VS_OK;
 }
 
+// Grid of a persistent kernel: SMs x resident CTAs per SM (queried once per
+// device and function; the first query happens outside any stream capture).
+static uint32_t persistent_grid(const void* fn, uint32_t threads, uint32_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, uint32_t> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find({dev, fn});
+  if (it != cache.end()) return it->second;
+  int sms = 0, per = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, (int)threads, smem) != cudaSuccess || per <= 0) per = 1;
+  const uint32_t g = (uint32_t)(sms * per);
+  cache[{dev, fn}] = g;
+  return g;
+}
+
 static int launch_pass(NttPass p, bool fwd, uint32_t n_cols, cudaStream_t st) {
   const uint32_t M = p.b - p.a + 1, T = M + p.c;
   PassFn fn = pass_fn(fwd, M, p.c);
   if (!fn) return set_error(VS_ERR_INVALID, "ntt: no kernel for pass shape M=%u C=%u", M, p.c);
-  const uint32_t tiles = 1u << (p.log_n - T);
-  fn<<<dim3(tiles, n_cols), 1u << (T - 5), 0, st>>>(p);
+  const uint32_t tile_bits = p.log_n - T;
+  const uint64_t total = (uint64_t)n_cols << tile_bits;
+  if (total > 0xFFFFFFFFull) return set_error(VS_ERR_INVALID, "ntt: %llu tiles", (unsigned long long)total);
+  const uint32_t smem = 8u << T;  // two tiles
+  VS_TRY(allow_smem((const void*)fn, smem));
+  const uint32_t threads = 1u << (T - 5);
+  const uint32_t grid = (uint32_t)std::min<uint64_t>(total, persistent_grid((const void*)fn, threads, smem));
+  fn<<<grid, threads, smem, st>>>(p, tile_bits, (uint32_t)total);
   VS_LAUNCHED("ntt_pass_kernel");
   return VS_OK;
 }
