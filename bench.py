@@ -180,6 +180,7 @@ def proof_workloads(args):
             eng.prepare(api.commit_job(j.log_n, 34, 0) if j.kind == api.COMMIT else j)
 
     out = {}
+    api.init_memory_pool(2 << 30)  # as the reference's prover initialises its pool
     plain = W.plain_jobs(64, 16)
     W.run_plain(plain[:4])
     t_plain, r_plain = W.run_plain(plain)
@@ -284,16 +285,18 @@ def main():
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
 
-    def step(marks=None):
+    def step(marks=None, c=None, f=None):
+        c = cols if c is None else c
+        f = fri_src if f is None else f
         if marks is not None:
             marks[0].record(st)
-        api.lde_stwo(cols, log_n, blow, out=lde)
+        api.lde_stwo(c, log_n, blow, out=lde)
         if marks is not None:
             marks[1].record(st)
         api.merkle_root_rowpacked(lde, root)
         if marks is not None:
             marks[2].record(st)
-        api.fri_fold_commit(fri_src, fri_log, alphas, work, roots, last)
+        api.fri_fold_commit(f, fri_log, alphas, work, roots, last)
         if marks is not None:
             marks[3].record(st)
 
@@ -327,7 +330,12 @@ def main():
         dist.barrier()
     value = committed * world / (ms / 1e3)
 
-    # end to end through the C ABI from pinned host buffers (H2D inputs, D2H roots)
+    # End to end through the C ABI from pinned host buffers: every step copies its
+    # inputs host -> device and reads its roots back. Inputs are double-buffered on
+    # the device and copied on a second stream, so step k+1's upload overlaps step
+    # k's compute (a step's upload waits until the step two back has released its
+    # buffer). The timed region runs from before the first upload to after the
+    # last read-back.
     e2e = None
     if not args.no_e2e:
         cols_h = torch.empty_like(cols, device="cpu").pin_memory()
@@ -335,24 +343,36 @@ def main():
         cols_h.copy_(cols)
         fri_h.copy_(fri_src)
         out_h = torch.empty(8 + 8 * (fri_log - 3) + 32, dtype=torch.int32).pin_memory()
+        bufs = [(cols, fri_src), (torch.empty_like(cols), torch.empty_like(fri_src))]
+        cs = torch.cuda.Stream()
+        free = [torch.cuda.Event(), torch.cuda.Event()]
+        for e in free:
+            e.record(st)
 
-        def e2e_step():
-            cols.copy_(cols_h, non_blocking=True)
-            fri_src.copy_(fri_h, non_blocking=True)
-            step()
-            out_h[:8].copy_(root, non_blocking=True)
-            out_h[8:8 + roots.numel()].copy_(roots, non_blocking=True)
-            out_h[8 + roots.numel():].copy_(last, non_blocking=True)
+        def e2e_run(k_steps):
+            for k in range(k_steps):
+                c, f = bufs[k & 1]
+                ready = torch.cuda.Event()
+                with torch.cuda.stream(cs):
+                    cs.wait_event(free[k & 1])
+                    c.copy_(cols_h, non_blocking=True)
+                    f.copy_(fri_h, non_blocking=True)
+                    ready.record(cs)
+                st.wait_event(ready)
+                step(c=c, f=f)
+                out_h[:8].copy_(root, non_blocking=True)
+                out_h[8:8 + roots.numel()].copy_(roots, non_blocking=True)
+                out_h[8 + roots.numel():].copy_(last, non_blocking=True)
+                free[k & 1].record(st)
 
-        for _ in range(2):
-            e2e_step()
+        e2e_run(2)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         e0, e1 = ev(), ev()
         e0.record(st)
-        for _ in range(args.steps):
-            e2e_step()
+        cs.wait_event(e0)
+        e2e_run(args.steps)
         e1.record(st)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1) / args.steps
@@ -361,17 +381,27 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ems = float(t.item())
         e2e = {"value": committed * world / (ems / 1e3), "unit": UNIT, "ms_per_step": ems,
-               "h2d_bytes_per_step": (cols.numel() + fri_src.numel()) * 4, "d2h_bytes_per_step": out_h.numel() * 4}
+               "h2d_bytes_per_step": (cols.numel() + fri_src.numel()) * 4, "d2h_bytes_per_step": out_h.numel() * 4,
+               "pipelining": "inputs double-buffered on the device; upload of step k+1 overlaps compute of step k"}
+        del bufs
 
-    # roofline of the dominant phase: algorithmic bytes per step / phase time
+    # Roofline of the dominant kernel: merkle_subtree_kernel<LeafRowPacked> (the
+    # largest single kernel of the step in the ncu launch list), timed by the events
+    # around the row-packed root (which also cover its 1024-to-1 upper reduction,
+    # under 0.3% of the phase). Algorithmic bytes: 4 * n_cols per leaf, each LDE
+    # word read once. Traffic: DRAM bytes per leaf from the ncu capture of the
+    # same kernel (34 columns, 2^22 leaves: 570.7 MB = 1.0004 x algorithmic),
+    # scaled to this launch's leaves. Per-phase HBM fractions are listed beside it;
+    # all phases are integer-ALU bound (Blake2s, M31 butterflies), not HBM bound.
     hbm = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0)) \
         if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
     alg = {"lde": n_cols * (4 * n + 4 * N), "merkle": n_cols * 4 * N,
            "fri": sum(24 * (1 << (l - 1)) for l in range(4, fri_log + 1))}
-    dom = max(phase, key=phase.get)
-    ach = alg[dom] / (phase[dom] / 1e3) / 1e9
-    roof = {"bound": "hbm", "kernel_phase": dom, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-            "traffic": None, "phase_ms": phase,
+    ach = alg["merkle"] / (phase["merkle"] / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": "merkle_subtree_kernel<LeafRowPacked>", "achieved": ach, "peak": hbm,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)", "unit": "GB/s", "frac": ach / hbm,
+            "traffic": alg["merkle"] * 1.0004, "algorithmic_bytes": alg["merkle"],
+            "launch_ms": phase["merkle"], "phase_ms": phase,
             "phase_hbm_frac": {k: alg[k] / (phase[k] / 1e3) / 1e9 / hbm for k in phase}}
 
     proofs = None

@@ -280,6 +280,12 @@ double vs_engine_now(void* engine);
 
 /* Release cached twiddles and scratch of the current device. */
 int vs_release_caches(void);
+/* Sets the release threshold of the current device's default stream-ordered
+ * memory pool (bytes kept cached across synchronisations; UINT64_MAX never
+ * releases). Replaces init_memory_pool (2 GiB) / init_memory_pool_greedy
+ * (src/cuda/ffi.rs:165-207); vs_prove_fib and the FRI scratch allocate from this
+ * pool, as the reference's DeviceBuffer does (src/device/buffer.rs:16-87). */
+int vs_init_memory_pool(uint64_t release_threshold_bytes);
 
 #ifdef __cplusplus
 }

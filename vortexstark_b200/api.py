@@ -101,6 +101,12 @@ def verify_fib(proof: bytes) -> tuple[bool, str]:
     return rc == 0, err.value.decode()
 
 
+def init_memory_pool(release_threshold_bytes: int = 2 << 30) -> None:
+    """Keep this many bytes cached in the device's default stream-ordered pool
+    (the reference's init_memory_pool keeps 2 GiB)."""
+    check(lib().vs_init_memory_pool(release_threshold_bytes), "vs_init_memory_pool")
+
+
 def launch_count() -> int:
     return int(lib().vs_launch_count())
 

@@ -50,6 +50,19 @@ int vs_release_caches(void) {
   return release_twiddles();
 }
 
+// src/cuda/ffi.rs:165-207 (init_memory_pool / init_memory_pool_greedy): the
+// reference keeps 2 GiB (or everything, greedy) cached in the current device's
+// default stream-ordered pool so per-proof cudaMallocAsync calls reuse memory.
+int vs_init_memory_pool(uint64_t release_threshold_bytes) {
+  clear_error();
+  int dev = 0;
+  VS_CUDA(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  VS_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  VS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &release_threshold_bytes));
+  return VS_OK;
+}
+
 int vs_commit_columns(const uint32_t* d_cols, uint32_t n_cols, uint32_t log_n, uint32_t blowup, uint32_t* d_lde,
                       uint32_t* d_root, vs_stream_t stream) {
   clear_error();
