@@ -220,6 +220,25 @@ def proof_workloads(args):
         "vs_plain": t_p / t_b, "vs_one_slot": t_one / t_b,
         "identical_plain_one_slot_batched": all(a == b[0] == c[0] for a, b, c in zip(r_p, r_one, r_b))}
 
+    # Single-proof latency at the sizes the reference publishes (prove_lean(1, 1, log_n)
+    # after a warm-up proof): the drop-in path and the graph-captured prover.
+    lat = {}
+    for L in args.prove_sizes:
+        api.prove_fib(1, 1, L)
+        t0 = time.perf_counter()
+        proof = api.prove_fib(1, 1, L)
+        t_plain = time.perf_counter() - t0
+        with api.Engine(1) as eng:
+            j = api.fib_job(L, 1, 1)
+            eng.prepare(j)
+            eng.wait(eng.submit(j))
+            t0 = time.perf_counter()
+            same = eng.wait(eng.submit(j))[0] == proof
+            t_graph = time.perf_counter() - t0
+        lat[str(L)] = {"vs_prove_fib_ms": t_plain * 1e3, "graph_prover_ms": t_graph * 1e3,
+                       "proof_bytes": len(proof), "identical": same, "verified": api.verify_fib(proof)[0]}
+    out["single_proof_latency"] = lat
+
     arrivals = W.served_arrivals(args.served_jobs)
     with api.Engine(args.slots, 150 * 10**9) as eng:
         prep(eng, [a[1] for a in arrivals])
@@ -246,6 +265,8 @@ def main():
     ap.add_argument("--no-proofs", action="store_true", help="skip the plain / batched / served proof runs")
     ap.add_argument("--slots", type=int, default=8, help="concurrent slots of the batched and served engines")
     ap.add_argument("--served-jobs", type=int, default=600)
+    ap.add_argument("--prove-sizes", type=int, nargs="*", default=[20, 24, 28],
+                    help="log_n of the single-proof latency runs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.cpu_log_n is None:
@@ -254,27 +275,23 @@ def main():
         return run_reference(args)
 
     import torch
-    import torch.distributed as dist
 
     import vortexstark_b200 as V
-    from vortexstark_b200 import api
+    from vortexstark_b200 import api, replicas
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = replicas.env()
     torch.cuda.set_device(local)
-    if world > 1:
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    replicas.init("nccl", timeout_s=120)
     V.lib()  # raises if the CUDA library is missing
 
     n_cols, log_n, blow, fri_log, N, committed = workload(args)
     n = 1 << log_n
     st = torch.cuda.current_stream()
     cols = torch.empty((n_cols, n), dtype=torch.int32, device="cuda")
-    api.fill_uniform_m31(cols, SEED, offset=rank * (n_cols << log_n))
+    api.fill_uniform_m31(cols, SEED, offset=replicas.input_offset(rank, n_cols << log_n))
     fri_src = torch.empty((4, 1 << fri_log), dtype=torch.int32, device="cuda")
-    api.fill_uniform_m31(fri_src, SEED + 1, offset=rank * (4 << fri_log))
+    api.fill_uniform_m31(fri_src, SEED + 1, offset=replicas.input_offset(rank, 4 << fri_log))
     alphas = splitmix_m31(SEED + 2, 0, 4 * (fri_log - 3))
     alphas = [alphas[4 * i:4 * i + 4] for i in range(fri_log - 3)]
     lde = torch.empty((n_cols, N), dtype=torch.int32, device="cuda")
@@ -303,8 +320,7 @@ def main():
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     marks = [[ev() for _ in range(4)] for _ in range(args.steps)]
     l0 = api.launch_count()
@@ -323,11 +339,8 @@ def main():
         phase["lde"] += m[0].elapsed_time(m[1]) / args.steps
         phase["merkle"] += m[1].elapsed_time(m[2]) / args.steps
         phase["fri"] += m[2].elapsed_time(m[3]) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    ms = replicas.max_over_ranks(ms, "cuda")
+    replicas.barrier()
     value = committed * world / (ms / 1e3)
 
     # End to end through the C ABI from pinned host buffers: every step copies its
@@ -367,8 +380,7 @@ def main():
 
         e2e_run(2)
         torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
+        replicas.barrier()
         e0, e1 = ev(), ev()
         e0.record(st)
         cs.wait_event(e0)
@@ -376,10 +388,7 @@ def main():
         e1.record(st)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1) / args.steps
-        if world > 1:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = replicas.max_over_ranks(ems, "cuda")
         e2e = {"value": committed * world / (ems / 1e3), "unit": UNIT, "ms_per_step": ems,
                "h2d_bytes_per_step": (cols.numel() + fri_src.numel()) * 4, "d2h_bytes_per_step": out_h.numel() * 4,
                "pipelining": "inputs double-buffered on the device; upload of step k+1 overlaps compute of step k"}
@@ -417,8 +426,7 @@ def main():
                 "config": config_json(args), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clk.summary(), "proofs": proofs}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finalize()
 
 
 if __name__ == "__main__":

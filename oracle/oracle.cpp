@@ -629,21 +629,61 @@ std::vector<uint32_t> fibonacci_trace(uint32_t a, uint32_t b, uint32_t log_n) {
 }
 
 // ------------------------------------------------------------------ prover
-template <class LeafFn>
-static std::vector<std::vector<Hash>> build_tree(uint64_t n, int threads, LeafFn leaf) {
-  std::vector<Hash> leaves(n);
-  parallel_for(n, threads, [&](uint64_t lo, uint64_t hi) { for (uint64_t i = lo; i < hi; i++) leaves[i] = leaf(i); });
-  std::vector<std::vector<Hash>> layers;
-  layers.push_back(std::move(leaves));
-  while (layers.back().size() > 1) {
-    const auto& prev = layers.back();
+// Merkle trees of the prover keep only the levels from 2^K-leaf tile roots up
+// (merkle.rs:804-842 keeps every level; the root and every auth path are the
+// same): a full tree of 2^30 leaves would take 64 GB of host memory. An auth
+// path recomputes its tile's leaves and inner levels from the leaf function.
+struct LeanTree {
+  uint32_t K = 0;                       // log2 leaves per tile
+  std::vector<std::vector<Hash>> up;    // up[0] = tile roots ... up.back() = {root}
+  std::function<Hash(uint64_t)> leaf;
+  const Hash& root() const { return up.back()[0]; }
+};
+static constexpr uint32_t LEAN_TILE_LOG = 10;
+
+static LeanTree build_tree(uint64_t n, int threads, std::function<Hash(uint64_t)> leaf) {
+  LeanTree t;
+  t.leaf = std::move(leaf);
+  uint32_t log_n = 0;
+  while ((1ull << log_n) < n) log_n++;
+  t.K = std::min(log_n, LEAN_TILE_LOG);
+  const uint64_t tile = 1ull << t.K, n_tiles = n >> t.K;
+  std::vector<Hash> roots(n_tiles);
+  parallel_for(n_tiles, threads, [&](uint64_t lo, uint64_t hi) {
+    std::vector<Hash> cur(tile);
+    for (uint64_t g = lo; g < hi; g++) {
+      for (uint64_t j = 0; j < tile; j++) cur[j] = t.leaf(g * tile + j);
+      for (uint64_t m = tile; m > 1; m >>= 1)
+        for (uint64_t j = 0; j < m / 2; j++) cur[j] = hash_node(cur[2 * j], cur[2 * j + 1]);
+      roots[g] = cur[0];
+    }
+  });
+  t.up.push_back(std::move(roots));
+  while (t.up.back().size() > 1) {
+    const auto& prev = t.up.back();
     std::vector<Hash> par(prev.size() / 2);
     parallel_for(par.size(), threads, [&](uint64_t lo, uint64_t hi) {
       for (uint64_t i = lo; i < hi; i++) par[i] = hash_node(prev[2 * i], prev[2 * i + 1]);
     });
-    layers.push_back(std::move(par));
+    t.up.push_back(std::move(par));
   }
-  return layers;
+  return t;
+}
+// Leaf-to-root siblings of leaf idx (merkle.rs:846-861 order).
+static std::vector<Hash> auth_path(const LeanTree& t, uint64_t idx) {
+  std::vector<Hash> path;
+  const uint64_t tile = 1ull << t.K, g = idx >> t.K;
+  std::vector<Hash> cur(tile);
+  for (uint64_t j = 0; j < tile; j++) cur[j] = t.leaf(g * tile + j);
+  uint64_t pos = idx & (tile - 1);
+  for (uint64_t m = tile; m > 1; m >>= 1) {
+    path.push_back(cur[pos ^ 1]);
+    for (uint64_t j = 0; j < m / 2; j++) cur[j] = hash_node(cur[2 * j], cur[2 * j + 1]);
+    pos >>= 1;
+  }
+  pos = g;
+  for (size_t l = 0; l + 1 < t.up.size(); l++) { path.push_back(t.up[l][pos ^ 1]); pos >>= 1; }
+  return path;
 }
 static Hash soa4_leaf(const std::vector<QM31>& v, uint64_t i) { return blake2s_words(v[i].v, 4); }
 static Q4 q4(const QM31& x) { return {x.v[0], x.v[1], x.v[2], x.v[3]}; }
@@ -665,7 +705,7 @@ StarkProof prove(uint32_t a, uint32_t b, uint32_t log_n, int threads) {
   // Step 4: trace tree (single column leaf, t = 4)
   auto trace_tree = build_tree(N, threads, [&](uint64_t i) { return leaf_hash_capped(&ev[i], 1); });
   StarkProof pf;
-  pf.trace_commitment = trace_tree.back()[0];
+  pf.trace_commitment = trace_tree.root();
 
   // Step 5: quotient
   Channel ch;
@@ -676,12 +716,13 @@ StarkProof prove(uint32_t a, uint32_t b, uint32_t log_n, int threads) {
     for (uint64_t i = lo; i < hi; i++) quot[i] = fib_quotient_at(ev.data(), N, i, alpha);
   });
   auto quot_tree = build_tree(N, threads, [&](uint64_t i) { return soa4_leaf(quot, i); });
-  pf.quotient_commitment = quot_tree.back()[0];
+  pf.quotient_commitment = quot_tree.root();
   ch.mix_digest(pf.quotient_commitment);
 
   // Step 7: FRI (prover.rs:1816-1904); twiddles per fri.rs:143-160
   std::vector<std::vector<QM31>> fri_evals;
-  std::vector<std::vector<std::vector<Hash>>> fri_trees;
+  fri_evals.reserve(64);  // leaf functions below index into it
+  std::vector<LeanTree> fri_trees;
   uint32_t cur_log = log_eval;
   {
     QM31 fa = ch.draw_felt();
@@ -689,10 +730,11 @@ StarkProof prove(uint32_t a, uint32_t b, uint32_t log_n, int threads) {
     std::vector<QM31> line(N / 2, QM31{{0, 0, 0, 0}});
     fold_circle_into_line(line.data(), quot.data(), tw.data(), fa, N / 2);
     cur_log--;
-    auto tree = build_tree(line.size(), threads, [&](uint64_t i) { return soa4_leaf(line, i); });
-    pf.fri_commitments.push_back(tree.back()[0]);
-    ch.mix_digest(tree.back()[0]);
     fri_evals.push_back(std::move(line));
+    const size_t l = fri_evals.size() - 1;
+    auto tree = build_tree(fri_evals[l].size(), threads, [&fri_evals, l](uint64_t i) { return soa4_leaf(fri_evals[l], i); });
+    pf.fri_commitments.push_back(tree.root());
+    ch.mix_digest(tree.root());
     fri_trees.push_back(std::move(tree));
   }
   while (cur_log > LOG_LAST_LAYER) {
@@ -702,10 +744,11 @@ StarkProof prove(uint32_t a, uint32_t b, uint32_t log_n, int threads) {
     std::vector<QM31> next(prev.size() / 2);
     fold_line(next.data(), prev.data(), tw.data(), fa, next.size());
     cur_log--;
-    auto tree = build_tree(next.size(), threads, [&](uint64_t i) { return soa4_leaf(next, i); });
-    pf.fri_commitments.push_back(tree.back()[0]);
-    ch.mix_digest(tree.back()[0]);
     fri_evals.push_back(std::move(next));
+    const size_t l = fri_evals.size() - 1;
+    auto tree = build_tree(fri_evals[l].size(), threads, [&fri_evals, l](uint64_t i) { return soa4_leaf(fri_evals[l], i); });
+    pf.fri_commitments.push_back(tree.root());
+    ch.mix_digest(tree.root());
     fri_trees.push_back(std::move(tree));
   }
   pf.fri_last_layer = fri_evals.back();

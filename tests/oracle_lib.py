@@ -369,10 +369,13 @@ def fib_trace(a, b, log_n) -> np.ndarray:
 
 def prove(a: int, b: int, log_n: int, threads: int = 0) -> bytes:
     threads = threads or (os.cpu_count() or 1)
-    n = lib().oracle_prove(a, b, log_n, threads, None, C.c_uint64(0))
-    buf = np.empty(n, np.uint8)
-    lib().oracle_prove(a, b, log_n, threads, ptr(buf), C.c_uint64(n))
-    return buf.tobytes()
+    cap = 32 << 20  # every proof up to log_n = 30 fits; proving twice would double the cost
+    buf = np.empty(cap, np.uint8)
+    n = lib().oracle_prove(a, b, log_n, threads, ptr(buf), C.c_uint64(cap))
+    if n > cap:
+        buf = np.empty(n, np.uint8)
+        lib().oracle_prove(a, b, log_n, threads, ptr(buf), C.c_uint64(n))
+    return buf[:n].tobytes()
 
 
 def verify(proof: bytes):

@@ -325,8 +325,7 @@ __device__ __forceinline__ void rounds_below_top(uint32_t* sm, const TileGeo& g,
 // blowup block q the forward layers [a, l-1] of the evaluation domain (tile
 // prefix hi = q) run on them and the result is written to dst block q.
 template <int M, int C>
-__global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_lde_top_kernel(NttPass inv, NttPass fwd, uint32_t B,
-                                                                      uint32_t* coeff_out, uint64_t coeff_stride) {
+__global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_lde_top_kernel(NttPass inv, NttPass fwd, uint32_t B) {
   using S = Tile<M, C>;
   constexpr int TOP = S::NR - 1;
   extern __shared__ uint32_t lde_sm[];
@@ -345,7 +344,6 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_lde_top_kernel(NttPas
     rstore<M, C, TOP>(v, cf);
   }
   __syncthreads();
-  if (coeff_out) tile_store<M, C>(cf, coeff_out + (uint64_t)blockIdx.y * coeff_stride, gi);
   uint32_t* dst = col_dst(fwd, blockIdx.y);
   for (uint32_t q = 0; q < (1u << B); q++) {
     TileGeo gf = gi;
@@ -365,7 +363,7 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_lde_top_kernel(NttPas
 // Launch tables: single / lower passes use C = 0 (T = M, 5 <= M <= 13); upper
 // passes use T = 13 (C = 13 - M, 1 <= M <= 11).
 using PassFn = void (*)(NttPass, uint32_t, uint32_t);
-using TopFn = void (*)(NttPass, NttPass, uint32_t, uint32_t*, uint64_t);
+using TopFn = void (*)(NttPass, NttPass, uint32_t);
 template <bool FWD, int M> PassFn pass_lo() { return ntt_pass_kernel<FWD, M, 0>; }
 template <bool FWD, int M> PassFn pass_hi() { return ntt_pass_kernel<FWD, M, 13 - M>; }
 template <int M> TopFn top_lo() { return ntt_lde_top_kernel<M, 0>; }
@@ -550,7 +548,7 @@ int ntt_transform(const NttColumns& io, uint32_t L, const NttTw& tw, bool fwd, c
 }
 
 int ntt_lde(const NttColumns& io, uint32_t l, uint32_t B, const NttTw& tw_inv, const NttTw& tw_fwd,
-            uint32_t* coeff_out, uint64_t coeff_stride, cudaStream_t st) {
+            cudaStream_t st) {
   if (l < 5) return set_error(VS_ERR_INVALID, "LDE needs log_n >= 5 (got %u)", l);
   if (io.src_cols || io.dst_cols) return set_error(VS_ERR_INVALID, "LDE takes strided columns");
   auto passes = plan_passes(l);
@@ -593,7 +591,7 @@ int ntt_lde(const NttColumns& io, uint32_t l, uint32_t B, const NttTw& tw_inv, c
     if (!fn) return set_error(VS_ERR_INVALID, "ntt: no LDE kernel for shape M=%u C=%u", M, r.c);
     const uint32_t smem = 8u << T;  // working tile + coefficient tile
     VS_TRY(allow_smem((const void*)fn, smem));
-    fn<<<dim3(1u << (l - T), io.n_cols), 1u << (T - 5), smem, st>>>(pi, pf, B, coeff_out, coeff_stride);
+    fn<<<dim3(1u << (l - T), io.n_cols), 1u << (T - 5), smem, st>>>(pi, pf, B);
     VS_LAUNCHED("ntt_lde_top_kernel");
   }
   // 3. forward passes below the top one over the whole evaluation domain
@@ -659,7 +657,7 @@ int lde_cached(int kind, const uint32_t* src, uint64_t src_stride, uint32_t* dst
     return VS_OK;
   }
   NttColumns io{src, dst, nullptr, nullptr, src_stride, dst_stride, n_cols};
-  return ntt_lde(io, l, B, ti, tf, nullptr, 0, st);
+  return ntt_lde(io, l, B, ti, tf, st);
 }
 
 // ------------------------------------------------------------------ bit reversal

@@ -50,7 +50,7 @@ int tw_for(int kind, uint32_t log_n, bool forward, NttTw* out, cudaStream_t st);
 int ntt_transform(const NttColumns& io, uint32_t log_n, const NttTw& tw, bool forward, cudaStream_t st);
 // interpolate(log_n) -> zero-pad -> evaluate(log_n + B); src is left untouched.
 int ntt_lde(const NttColumns& io, uint32_t log_n, uint32_t B, const NttTw& tw_inv, const NttTw& tw_fwd,
-            uint32_t* coeff_out, uint64_t coeff_stride, cudaStream_t st);
+            cudaStream_t st);
 int lde_cached(int kind, const uint32_t* src, uint64_t src_stride, uint32_t* dst, uint64_t dst_stride,
                uint32_t n_cols, uint32_t log_n, uint32_t B, cudaStream_t st);
 
