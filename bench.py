@@ -240,11 +240,13 @@ def proof_workloads(args):
     out["single_proof_latency"] = lat
 
     arrivals = W.served_arrivals(args.served_jobs)
-    with api.Engine(args.slots, 150 * 10**9) as eng:
-        prep(eng, [a[1] for a in arrivals])
-        recs = W.run_served(eng, arrivals)
-    out["served"] = dict(W.summarize_served(recs), workload="Poisson 200 jobs/s: Fibonacci 16/20/24 (0.5/0.3/0.2) "
-                         "and 34-col commits 18/20/22", slots=args.slots, hbm_budget_gb=150)
+    for key, by_size in (("served", True), ("served_fifo_priority", False)):
+        with api.Engine(args.slots, 150 * 10**9, size_priority=by_size) as eng:
+            prep(eng, [a[1] for a in arrivals])
+            recs = W.run_served(eng, arrivals)
+        out[key] = dict(W.summarize_served(recs), workload="Poisson 200 jobs/s: Fibonacci 16/20/24 (0.5/0.3/0.2) "
+                        "and 34-col commits 18/20/22", slots=args.slots, hbm_budget_gb=150,
+                        stream_priority="by job size, smallest first" if by_size else "equal for all jobs")
     return out
 
 

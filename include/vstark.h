@@ -267,6 +267,13 @@ typedef struct {
   double t_submit, t_start, t_end;
 } vs_job_result;
 int vs_engine_create(uint32_t n_slots, uint64_t hbm_budget_bytes, void** engine);
+/* As vs_engine_create with flags: VS_ENGINE_FIFO_PRIORITY runs every job at the
+ * same stream priority; by default (flags 0, and vs_engine_create) jobs run at
+ * one of three CUDA stream priorities by working-set size, smallest first, which
+ * shortens small jobs' latency at some cost to large jobs' tails. Results are the
+ * same either way. */
+#define VS_ENGINE_FIFO_PRIORITY 1u
+int vs_engine_create_ex(uint32_t n_slots, uint64_t hbm_budget_bytes, uint32_t flags, void** engine);
 int vs_engine_destroy(void* engine);
 /* Builds the workspace for this job shape in every slot (outside any timing). */
 int vs_engine_prepare(void* engine, const vs_job* shape);

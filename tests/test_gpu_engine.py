@@ -60,9 +60,12 @@ def commit_root_oracle(log_n, n_cols, seed):
     return O.merkle_root_rowpacked(O.stwo_lde_columns(cols, log_n, 2, threads=8), threads=8).tobytes()
 
 
-def run_engine(L, jobs, slots, budget=0):
+def run_engine(L, jobs, slots, budget=0, flags=None):
     eng = C.c_void_p()
-    V.check(L.vs_engine_create(slots, budget, C.byref(eng)), "vs_engine_create")
+    if flags is None:
+        V.check(L.vs_engine_create(slots, budget, C.byref(eng)), "vs_engine_create")
+    else:
+        V.check(L.vs_engine_create_ex(slots, budget, flags, C.byref(eng)), "vs_engine_create_ex")
     try:
         tickets = []
         for j in jobs:
@@ -125,3 +128,13 @@ def test_engine_rejects_bad_jobs(L):
         assert L.vs_engine_wait(eng, t.value, C.byref(r), None, 0) == 1 and r.status == 1
     finally:
         L.vs_engine_destroy(eng)
+
+
+def test_engine_priority_policy_does_not_change_results(L):
+    """Size-based stream priorities (default) and equal priorities give the same bytes."""
+    jobs = mixed_jobs()
+    by_size = run_engine(L, jobs, slots=6, flags=0)
+    fifo = run_engine(L, jobs, slots=6, flags=1)
+    assert [r[0] for r in by_size] == [r[0] for r in fifo]
+    eng = C.c_void_p()
+    assert L.vs_engine_create_ex(2, 0, 0x80, C.byref(eng)) == 1  # unknown flag rejected

@@ -137,9 +137,11 @@ def commit_job(log_n: int, n_cols: int, seed: int) -> Job:
 class Engine:
     """Slots of concurrent provers with FIFO admission against an HBM budget."""
 
-    def __init__(self, slots: int, hbm_budget_bytes: int = 0):
+    def __init__(self, slots: int, hbm_budget_bytes: int = 0, size_priority: bool = True):
+        """size_priority: run small jobs on higher-priority CUDA streams (VS_ENGINE_FIFO_PRIORITY off)."""
         self.h = C.c_void_p()
-        check(lib().vs_engine_create(slots, hbm_budget_bytes, C.byref(self.h)), "vs_engine_create")
+        flags = 0 if size_priority else 1
+        check(lib().vs_engine_create_ex(slots, hbm_budget_bytes, flags, C.byref(self.h)), "vs_engine_create_ex")
         self._buf = (C.c_uint8 * PROOF_CAP)()
 
     def prepare(self, job: Job) -> None:

@@ -50,9 +50,17 @@ uint64_t commit_bytes(uint32_t log_n, uint32_t n_cols) {
   return (uint64_t)n_cols * (n + N) * 4 + merkle_scratch_words(N) * 4 + 64;
 }
 
+// Jobs run at one of three stream priorities by working-set size (small jobs
+// first), so a small proof admitted beside large ones is not stuck behind their
+// queued kernels. Priority changes only scheduling, never a result.
+constexpr int kPrioLevels = 3;
+int prio_level(uint64_t job_bytes) {
+  return job_bytes <= (64ull << 20) ? 0 : (job_bytes <= (512ull << 20) ? 1 : 2);
+}
+
 struct Slot {
   int device = 0;
-  cudaStream_t st = nullptr;
+  cudaStream_t st[kPrioLevels] = {};
   std::unordered_map<uint64_t, std::unique_ptr<GraphProver>> provers;
   std::unordered_map<uint64_t, std::unique_ptr<CommitWs>> commits;
   std::thread th;
@@ -71,6 +79,8 @@ struct Result {
 
 struct Engine {
   int device = 0;
+  int prio_greatest = 0, prio_least = 0;  // CUDA stream priority range (greatest is numerically lowest)
+  bool by_size = true;                     // false: every job at the least priority
   uint64_t budget = 0, reserved = 0, next_ticket = 1;
   Clock::time_point t0 = Clock::now();
   std::vector<std::unique_ptr<Slot>> slots;
@@ -82,6 +92,10 @@ struct Engine {
   uint64_t in_flight = 0;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+  int priority(int level) const {  // level 0 -> greatest priority, last level -> least
+    return prio_greatest + (prio_least - prio_greatest) * level / (kPrioLevels - 1);
+  }
+  int level_of(uint64_t bytes) const { return by_size ? prio_level(bytes) : kPrioLevels - 1; }
 
   int prover_for(Slot& s, uint32_t log_n, GraphProver** out) {
     vs_job j{};
@@ -90,7 +104,7 @@ struct Engine {
     auto& p = s.provers[shape_key(j)];
     if (!p) {
       auto np = std::make_unique<GraphProver>();
-      VS_TRY(np->init(log_n));
+      VS_TRY(np->init(log_n, priority(level_of(job_bytes(j)))));
       p = std::move(np);
     }
     *out = p.get();
@@ -110,8 +124,9 @@ struct Engine {
       VS_CUDA(cudaMallocHost(&w->h_root, 32));
       w->bytes = commit_bytes(j.log_n, w->capacity);
       const TwiddleSet* t = nullptr;
-      VS_TRY(get_twiddles(TW_STWO, j.log_n, &t, s.st));
-      VS_TRY(get_twiddles(TW_STWO, j.log_n + 2, &t, s.st));
+      cudaStream_t st = s.st[level_of(commit_bytes(j.log_n, j.n_cols))];
+      VS_TRY(get_twiddles(TW_STWO, j.log_n, &t, st));
+      VS_TRY(get_twiddles(TW_STWO, j.log_n + 2, &t, st));
       c = std::move(w);
     }
     *out = c.get();
@@ -136,11 +151,12 @@ struct Engine {
     CommitWs* w = nullptr;
     VS_TRY(commit_for(s, j, &w));
     const uint64_t n = 1ull << j.log_n, N = n << 2;
-    VS_TRY(vs_fill_uniform_m31(w->cols, (uint64_t)j.n_cols * n, j.seed, 0, (vs_stream_t)s.st));
-    VS_TRY(lde_cached(TW_STWO, w->cols, n, w->lde, N, j.n_cols, j.log_n, 2, s.st));
-    VS_TRY(merkle_root(LeafRowPacked{w->lde, N, j.n_cols}, N, w->root, s.st, w->scratch));
-    VS_CUDA(cudaMemcpyAsync(w->h_root, w->root, 32, cudaMemcpyDeviceToHost, s.st));
-    VS_CUDA(cudaStreamSynchronize(s.st));
+    cudaStream_t st = s.st[level_of(commit_bytes(j.log_n, j.n_cols))];
+    VS_TRY(vs_fill_uniform_m31(w->cols, (uint64_t)j.n_cols * n, j.seed, 0, (vs_stream_t)st));
+    VS_TRY(lde_cached(TW_STWO, w->cols, n, w->lde, N, j.n_cols, j.log_n, 2, st));
+    VS_TRY(merkle_root(LeafRowPacked{w->lde, N, j.n_cols}, N, w->root, st, w->scratch));
+    VS_CUDA(cudaMemcpyAsync(w->h_root, w->root, 32, cudaMemcpyDeviceToHost, st));
+    VS_CUDA(cudaStreamSynchronize(st));
     out.assign((uint8_t*)w->h_root, (uint8_t*)w->h_root + 32);
     return VS_OK;
   }
@@ -195,17 +211,29 @@ using namespace vs;
 extern "C" {
 
 int vs_engine_create(uint32_t n_slots, uint64_t hbm_budget_bytes, void** out) {
+  return vs_engine_create_ex(n_slots, hbm_budget_bytes, 0, out);
+}
+
+int vs_engine_create_ex(uint32_t n_slots, uint64_t hbm_budget_bytes, uint32_t flags, void** out) {
   clear_error();
   if (!out || n_slots == 0 || n_slots > 64) return set_error(VS_ERR_INVALID, "vs_engine_create: 1..64 slots");
+  if (flags & ~VS_ENGINE_FIFO_PRIORITY) return set_error(VS_ERR_INVALID, "vs_engine_create_ex: unknown flags %#x", flags);
   auto* e = new Engine();
+  e->by_size = !(flags & VS_ENGINE_FIFO_PRIORITY);
   VS_CUDA(cudaGetDevice(&e->device));
+  VS_CUDA(cudaDeviceGetStreamPriorityRange(&e->prio_least, &e->prio_greatest));
   e->budget = hbm_budget_bytes ? hbm_budget_bytes : ~0ull;
   for (uint32_t i = 0; i < n_slots; i++) {
     auto s = std::make_unique<Slot>();
     s->device = e->device;
-    if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
-      delete e;
-      return set_error(VS_ERR_CUDA, "vs_engine_create: stream");
+    for (int l = 0; l < kPrioLevels; l++) {
+      if (cudaStreamCreateWithPriority(&s->st[l], cudaStreamNonBlocking, e->priority(l)) != cudaSuccess) {
+        for (auto& o : e->slots)
+          for (cudaStream_t x : o->st) if (x) cudaStreamDestroy(x);
+        for (cudaStream_t x : s->st) if (x) cudaStreamDestroy(x);
+        delete e;
+        return set_error(VS_ERR_CUDA, "vs_engine_create: stream");
+      }
     }
     e->slots.push_back(std::move(s));
   }
@@ -228,7 +256,8 @@ int vs_engine_destroy(void* h) {
   for (auto& s : e->slots) {
     s->provers.clear();
     s->commits.clear();
-    if (s->st) cudaStreamDestroy(s->st);
+    for (cudaStream_t x : s->st)
+      if (x) cudaStreamDestroy(x);
   }
   delete e;
   return VS_OK;

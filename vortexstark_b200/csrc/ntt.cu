@@ -266,32 +266,34 @@ __device__ __forceinline__ uint32_t* col_dst(const NttPass& p, uint32_t c) {
   return p.dst_cols ? p.dst_cols[c] : p.dst + (uint64_t)c * p.dst_stride;
 }
 
-// One pass over work items w = column * 2^tile_bits + tile, strided by the grid.
+// One pass over work items w = tile * n_cols + column, strided by the grid:
+// tile-major, so the columns of one tile range run back to back and the twiddles
+// of that range (the low layers' tables outgrow L2 at 2^26 points) are fetched
+// from HBM once and then hit L2 for the other columns.
 // Per item: NR register rounds (forward: top round first) on the shared tile,
 // then the tile is stored; the next item's tile is already in flight into the
 // other buffer. The inverse scale is folded into the last round of the last
 // inverse pass. Every thread commits one copy group per iteration (empty at the
 // end), so "wait until one group is pending" always means "this tile landed".
 template <bool FWD, int M, int C>
-__global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_pass_kernel(NttPass p, uint32_t tile_bits,
+__global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_pass_kernel(NttPass p, uint32_t n_cols,
                                                                       uint32_t total) {
   using S = Tile<M, C>;
   extern __shared__ __align__(16) uint32_t pass_sm[];
   uint32_t w = blockIdx.x;
   if (w >= total) return;
-  const uint32_t tmask = (1u << tile_bits) - 1;
-  tile_load_async<M, C>(pass_sm, col_src(p, w >> tile_bits), tile_geo<M, C>(p.a, w & tmask), p.src_mask);
+  tile_load_async<M, C>(pass_sm, col_src(p, w % n_cols), tile_geo<M, C>(p.a, w / n_cols), p.src_mask);
   cp_async_commit();
   for (uint32_t it = 0; w < total; it++, w += gridDim.x) {
     uint32_t* sm = pass_sm + (it & 1) * S::SIZE;
     const uint32_t nw = w + gridDim.x;
     if (nw < total)
-      tile_load_async<M, C>(pass_sm + ((it + 1) & 1) * S::SIZE, col_src(p, nw >> tile_bits),
-                            tile_geo<M, C>(p.a, nw & tmask), p.src_mask);
+      tile_load_async<M, C>(pass_sm + ((it + 1) & 1) * S::SIZE, col_src(p, nw % n_cols),
+                            tile_geo<M, C>(p.a, nw / n_cols), p.src_mask);
     cp_async_commit();
     cp_async_wait1();
     __syncthreads();
-    const TileGeo g = tile_geo<M, C>(p.a, w & tmask);
+    const TileGeo g = tile_geo<M, C>(p.a, w / n_cols);
 #pragma unroll
     for (int rr = 0; rr < S::NR; rr++) {
       const uint32_t sc = (!FWD && rr == S::NR - 1) ? p.scale : 0u;
@@ -302,7 +304,7 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_pass_kernel(NttPass p
       }
       __syncthreads();
     }
-    tile_store<M, C>(sm, col_dst(p, w >> tile_bits), g);
+    tile_store<M, C>(sm, col_dst(p, w % n_cols), g);
     __syncthreads();  // this buffer is refilled by the next iteration's prefetch
   }
 }
@@ -494,7 +496,7 @@ static int launch_pass(NttPass p, bool fwd, uint32_t n_cols, cudaStream_t st) {
   VS_TRY(allow_smem((const void*)fn, smem));
   const uint32_t threads = 1u << (T - 5);
   const uint32_t grid = (uint32_t)std::min<uint64_t>(total, persistent_grid((const void*)fn, threads, smem));
-  fn<<<grid, threads, smem, st>>>(p, tile_bits, (uint32_t)total);
+  fn<<<grid, threads, smem, st>>>(p, n_cols, (uint32_t)total);
   VS_LAUNCHED("ntt_pass_kernel");
   return VS_OK;
 }

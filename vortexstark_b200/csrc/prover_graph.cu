@@ -306,14 +306,14 @@ struct GraphProver::Impl {
     return VS_OK;
   }
 
-  int setup(uint32_t ln) {
+  int setup(uint32_t ln, int priority) {
     log_n = ln;
     log_eval = ln + BLOWUP_BITS;
     n = 1ull << ln;
     N = 1ull << log_eval;
     nf = log_eval - LOG_LAST_LAYER;
     VS_CUDA(cudaGetDevice(&device));
-    VS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    VS_CUDA(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, priority));
     VS_CUDA(cudaMallocHost((void**)&h_ab, 16));
     VS_TRY(alloc(&d_ab, 4));
     VS_TRY(alloc(&d_trace, n));
@@ -462,9 +462,9 @@ struct GraphProver::Impl {
 
 GraphProver::GraphProver() : impl(new Impl) {}
 GraphProver::~GraphProver() = default;
-int GraphProver::init(uint32_t log_n) {
+int GraphProver::init(uint32_t log_n, int priority) {
   if (log_n < 4 || log_n + BLOWUP_BITS > 30) return set_error(VS_ERR_INVALID, "log_n %u outside [4, 28]", log_n);
-  return impl->setup(log_n);
+  return impl->setup(log_n, priority);
 }
 uint32_t GraphProver::log_n() const { return impl->log_n; }
 int GraphProver::device() const { return impl->device; }

@@ -13,7 +13,9 @@ class GraphProver {
   GraphProver();
   ~GraphProver();
   // Allocates the workspace on the current device, builds twiddles and captures the graph.
-  int init(uint32_t log_n);
+  // The proof runs on a stream of the given CUDA priority (0 = default; lower
+  // numbers are served first when several streams have work queued).
+  int init(uint32_t log_n, int priority = 0);
   // Starts a proof (one in flight per instance); finish() waits and serialises KRAK v1.
   int launch(uint32_t a, uint32_t b);
   int finish(uint32_t a, uint32_t b, std::vector<uint8_t>& out);
