@@ -30,6 +30,11 @@ from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+# The slot engine keeps up to 24 streams busy at once (8 slots x 3 priorities).
+# With the default 8 hardware queues, streams share queues and a small job can
+# wait behind a large job's kernels; 32 gives every stream its own queue. Read by
+# CUDA at context creation, so it is set before torch touches the GPU.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 SEED = 0x56530001
 METRIC = "committed M31 elems/s & proofs/s batched vs plain on 1 B200; p50/p99 latency"
@@ -193,7 +198,9 @@ def proof_workloads(args):
     out["plain"] = {"workload": "64 Fibonacci proofs, log_n=16, a0=1, a1 seeded; vs_prove_fib one at a time",
                     "proofs_per_s": len(plain) / t_plain, "p50_ms": W.percentile(lat, 0.5),
                     "p99_ms": W.percentile(lat, 0.99), "verified": ok}
-    with api.Engine(args.slots) as eng:
+    # Batches are throughput work: every job at the same stream priority (the
+    # size-priority default is the serving policy, measured below).
+    with api.Engine(args.slots, size_priority=False) as eng:
         prep(eng, plain)
         W.run_list(eng, plain[:16], sequential=False)
         t_e, r_e = W.run_list(eng, plain, sequential=False)
@@ -205,10 +212,10 @@ def proof_workloads(args):
     jobs = W.batched_jobs(64)
     W.run_plain(W.shapes(jobs))
     t_p, r_p = W.run_plain(jobs)
-    with api.Engine(1) as one:
+    with api.Engine(1, size_priority=False) as one:
         prep(one, jobs)
         t_one, r_one = W.run_list(one, jobs, sequential=True)
-    with api.Engine(args.slots) as eng:
+    with api.Engine(args.slots, size_priority=False) as eng:
         prep(eng, jobs)
         W.run_list(eng, jobs[:8], sequential=False)
         t_b, r_b = W.run_list(eng, jobs, sequential=False)
@@ -345,6 +352,27 @@ def main():
     replicas.barrier()
     value = committed * world / (ms / 1e3)
 
+    # The reference-faithful three-tree form of the same commitment (its Cairo
+    # prover commits 34 columns as trees of 16 / 15 / 3 columns with the native
+    # leaf of at most 16 words), over the same LDE, beside the row-packed root.
+    groups = [(a, min(a + 16, n_cols)) for a in range(0, n_cols, 16)] if n_cols != 34 else [(0, 16), (16, 31), (31, 34)]
+    roots3 = torch.zeros((len(groups), 8), dtype=torch.int32, device="cuda")
+
+    def three_tree():
+        for i, (a, b) in enumerate(groups):
+            api.merkle_root_capped(lde[a:b], roots3[i])
+
+    three_tree()
+    torch.cuda.synchronize()
+    m0, m1 = ev(), ev()
+    m0.record(st)
+    for _ in range(args.steps):
+        three_tree()
+    m1.record(st)
+    torch.cuda.synchronize()
+    three = {"groups": "/".join(str(b - a) for a, b in groups), "ms": m0.elapsed_time(m1) / args.steps,
+             "row_packed_root_ms": phase["merkle"]}
+
     # End to end through the C ABI from pinned host buffers: every step copies its
     # inputs host -> device and reads its roots back. Inputs are double-buffered on
     # the device and copied on a second stream, so step k+1's upload overlaps step
@@ -426,7 +454,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic (seeded SplitMix64 uniform M31)",
                 "config": config_json(args), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": clk.summary(), "proofs": proofs}
+                "gpu_launches": launches, "clocks": clk.summary(), "three_tree_commit": three,
+                "proofs": proofs}
         print(json.dumps(line), flush=True)
     replicas.finalize()
 

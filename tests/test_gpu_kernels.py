@@ -309,3 +309,17 @@ def test_commit_columns(L, log_n, n_cols):
     exp_lde = O.stwo_lde_columns(cols, log_n, 2, threads=8)
     assert np.array_equal(host(lde).reshape(n_cols, -1), exp_lde)
     assert np.array_equal(host(root), O.merkle_root_rowpacked(exp_lde, threads=8))
+
+
+def test_three_tree_commit_16_15_3(L):
+    """The reference's three-tree commitment of 34 LDE columns (16 / 15 / 3 columns,
+    native leaf) through api.merkle_root_capped on row slices of one LDE tensor."""
+    from vortexstark_b200 import api
+    log_n = 11
+    cols = O.seeded_m31(0x5653, 34 << log_n).reshape(34, -1)
+    lde = dev(O.stwo_lde_columns(cols, log_n, 2, threads=8).reshape(34, -1))
+    for a, b in ((0, 16), (16, 31), (31, 34)):
+        root = zeros(8)
+        api.merkle_root_capped(lde[a:b], root)
+        torch.cuda.synchronize()
+        assert np.array_equal(host(root), O.merkle_root_capped(host(lde[a:b]).reshape(b - a, -1), threads=8))

@@ -55,6 +55,16 @@ def merkle_root_rowpacked(cols: torch.Tensor, root: torch.Tensor, stream=None):
           "vs_merkle_root_rowpacked")
 
 
+def merkle_root_capped(cols: torch.Tensor, root: torch.Tensor, stream=None):
+    """Root over leaves of the first min(n_cols, 16) columns (the reference's native leaf)."""
+    n_cols, n = cols.shape
+    stride = cols.stride(0)
+    if cols.stride(1) != 1 or not cols.is_cuda or cols.dtype != torch.int32:
+        raise TypeError("expected int32 CUDA rows with unit stride")
+    check(lib().vs_merkle_root_capped(cols.data_ptr(), stride, n_cols, n.bit_length() - 1, _ptr(root),
+                                      _stream(stream)), "vs_merkle_root_capped")
+
+
 def fri_fold_commit(src: torch.Tensor, log_n: int, alphas, work: torch.Tensor, roots: torch.Tensor,
                     last: torch.Tensor, stream=None):
     """src: (4, 2^log_n) SoA4 QM31; alphas: (log_n - 3) x 4 host words."""

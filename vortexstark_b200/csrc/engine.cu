@@ -4,6 +4,8 @@
 // the head job only when the bytes reserved by running jobs plus the head job's
 // working set fit the HBM budget, so jobs that arrive while others run are
 // admitted as slots and memory free up, and their work overlaps on the device.
+// Under the default size-priority policy small jobs also run on higher-priority
+// streams, and a quarter of the slots take only small jobs (oldest first).
 // Each job's result depends only on the job (never on what ran beside it).
 #include <chrono>
 #include <condition_variable>
@@ -60,6 +62,7 @@ int prio_level(uint64_t job_bytes) {
 
 struct Slot {
   int device = 0;
+  bool small_only = false;  // takes only jobs of priority level 0
   cudaStream_t st[kPrioLevels] = {};
   std::unordered_map<uint64_t, std::unique_ptr<GraphProver>> provers;
   std::unordered_map<uint64_t, std::unique_ptr<CommitWs>> commits;
@@ -143,7 +146,7 @@ struct Engine {
     if (j.kind == VS_JOB_FIB) {
       GraphProver* p = nullptr;
       VS_TRY(prover_for(s, j.log_n, &p));
-      VS_TRY(p->launch(j.a, j.b));
+      VS_TRY(p->launch(j.a, j.b, s.st[level_of(job_bytes(j))]));
       return p->finish(j.a, j.b, out);
     }
     if (j.kind != VS_JOB_COMMIT || j.n_cols == 0 || j.log_n < 2 || j.log_n + 2 > 30)
@@ -169,15 +172,27 @@ struct Engine {
       uint64_t bytes = 0;
       {
         std::unique_lock<std::mutex> lk(mu);
+        auto pick = queue.end();
         cv_work.wait(lk, [&] {
           if (stop) return true;
-          if (queue.empty()) return false;
-          const vs_job& head = results[queue.front()].job;
-          return reserved + job_bytes(head) <= budget || reserved == 0;  // an oversized job runs alone
+          auto fits = [&](const vs_job& j) { return reserved + job_bytes(j) <= budget || reserved == 0; };
+          pick = queue.end();
+          if (s->small_only) {  // the oldest small job, wherever it is in the queue
+            for (auto it = queue.begin(); it != queue.end(); ++it) {
+              const vs_job& j = results[*it].job;
+              if (prio_level(job_bytes(j)) == 0) {
+                if (fits(j)) pick = it;
+                break;
+              }
+            }
+          } else if (!queue.empty() && fits(results[queue.front()].job)) {  // FIFO; an oversized job runs alone
+            pick = queue.begin();
+          }
+          return pick != queue.end();
         });
         if (stop) return;
-        ticket = queue.front();
-        queue.pop_front();
+        ticket = *pick;
+        queue.erase(pick);
         job = results[ticket].job;
         bytes = job_bytes(job);
         reserved += bytes;
@@ -237,6 +252,10 @@ int vs_engine_create_ex(uint32_t n_slots, uint64_t hbm_budget_bytes, uint32_t fl
     }
     e->slots.push_back(std::move(s));
   }
+  // With size priorities, a quarter of the slots (from 4 slots up) take only
+  // small jobs, so a small job never queues behind large ones for a slot.
+  if (e->by_size)
+    for (uint32_t i = n_slots - n_slots / 4; i < n_slots; i++) e->slots[i]->small_only = true;
   for (auto& s : e->slots) s->th = std::thread(&Engine::worker, e, s.get());
   *out = e;
   return VS_OK;
@@ -269,6 +288,7 @@ int vs_engine_prepare(void* h, const vs_job* shape) {
   if (!e || !shape) return set_error(VS_ERR_INVALID, "vs_engine_prepare: null");
   std::lock_guard<std::mutex> lk(e->mu);  // workers idle on the queue; preparation is not concurrent with jobs
   for (auto& s : e->slots) {
+    if (s->small_only && prio_level(e->job_bytes(*shape)) != 0) continue;  // never runs there
     if (shape->kind == VS_JOB_FIB) {
       GraphProver* p = nullptr;
       VS_TRY(e->prover_for(*s, shape->log_n, &p));
@@ -296,7 +316,7 @@ int vs_engine_submit(void* h, const vs_job* job, uint64_t* ticket) {
     e->in_flight++;
     *ticket = t;
   }
-  e->cv_work.notify_one();
+  e->cv_work.notify_all();  // slots differ in what they may take: wake them all
   return VS_OK;
 }
 

@@ -12,8 +12,8 @@
 // for coalescing) into shared memory, runs its layers as register rounds of up
 // to five layers (32 elements per thread, no barrier inside a round) and writes
 // the tile back once. The shared tile uses a 16-byte-chunk XOR swizzle (swz)
-// that keeps every round's access pattern bank-conflict free. Pass kernels are
-// persistent (resident CTAs x SMs) and double-buffer their tiles: the next tile
+// that keeps every round's access pattern bank-conflict free. Pass kernels loop
+// over up to 8 tiles per CTA and double-buffer them: the next tile
 // streams in with 16-byte cp.async copies while the current one is transformed,
 // so HBM latency hides behind the integer work. A 2^24-point transform is two
 // HBM round trips instead of the reference's 24 per-layer launches.
@@ -494,8 +494,14 @@ static int launch_pass(NttPass p, bool fwd, uint32_t n_cols, cudaStream_t st) {
   if (total > 0xFFFFFFFFull) return set_error(VS_ERR_INVALID, "ntt: %llu tiles", (unsigned long long)total);
   const uint32_t smem = 8u << T;  // two tiles
   VS_TRY(allow_smem((const void*)fn, smem));
+  // At most kItemsPerCta tiles per CTA: the prefetch pipeline still hides the
+  // loads, and CTAs retire every few tens of microseconds, so kernels of
+  // higher-priority streams (small jobs beside a large one) get SMs promptly
+  // instead of waiting for a whole-GPU persistent kernel to end.
+  constexpr uint64_t kItemsPerCta = 8;
   const uint32_t threads = 1u << (T - 5);
-  const uint32_t grid = (uint32_t)std::min<uint64_t>(total, persistent_grid((const void*)fn, threads, smem));
+  const uint64_t resident = persistent_grid((const void*)fn, threads, smem);
+  const uint32_t grid = (uint32_t)std::min<uint64_t>(total, std::max(resident, (total + kItemsPerCta - 1) / kItemsPerCta));
   fn<<<grid, threads, smem, st>>>(p, n_cols, (uint32_t)total);
   VS_LAUNCHED("ntt_pass_kernel");
   return VS_OK;

@@ -239,6 +239,7 @@ struct GraphProver::Impl {
   uint64_t n = 0, N = 0;
   int device = 0;
   cudaStream_t st = nullptr;
+  cudaStream_t running = nullptr;  // stream of the proof in flight
   std::vector<void*> allocs;
   uint32_t *d_ab = nullptr, *h_ab = nullptr, *d_trace = nullptr, *d_eval = nullptr, *d_alpha = nullptr,
            *d_qidx = nullptr, *d_arena = nullptr, *h_arena = nullptr;
@@ -254,9 +255,10 @@ struct GraphProver::Impl {
   cudaGraph_t graph = nullptr;
 
   ~Impl() {
+    if (running) cudaStreamSynchronize(running);
+    if (st) cudaStreamSynchronize(st);
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
-    if (st) cudaStreamSynchronize(st);
     for (void* p : allocs) cudaFree(p);
     if (h_arena) cudaFreeHost(h_arena);
     if (h_ab) cudaFreeHost(h_ab);
@@ -479,15 +481,18 @@ int GraphProver::launch(uint32_t a, uint32_t b) {
   if (a >= h::P || b >= h::P) return set_error(VS_ERR_INVALID, "public inputs must be canonical M31");
   impl->h_ab[0] = a;
   impl->h_ab[1] = b;
-  VS_CUDA(cudaGraphLaunch(impl->exec, impl->st));
+  impl->running = on ? on : impl->st;
+  VS_CUDA(cudaGraphLaunch(impl->exec, impl->running));
   return VS_OK;
 }
 int GraphProver::finish(uint32_t a, uint32_t b, std::vector<uint8_t>& out) {
-  VS_CUDA(cudaStreamSynchronize(impl->st));
+  VS_CUDA(cudaStreamSynchronize(impl->running ? impl->running : impl->st));
   impl->serialize(a, b, out);
   return VS_OK;
 }
-bool GraphProver::busy() const { return cudaStreamQuery(impl->st) == cudaErrorNotReady; }
+bool GraphProver::busy() const {
+  return cudaStreamQuery(impl->running ? impl->running : impl->st) == cudaErrorNotReady;
+}
 
 }  // namespace vs
 

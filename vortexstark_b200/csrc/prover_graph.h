@@ -16,8 +16,9 @@ class GraphProver {
   // The proof runs on a stream of the given CUDA priority (0 = default; lower
   // numbers are served first when several streams have work queued).
   int init(uint32_t log_n, int priority = 0);
-  // Starts a proof (one in flight per instance); finish() waits and serialises KRAK v1.
-  int launch(uint32_t a, uint32_t b);
+  // Starts a proof (one in flight per instance) on `on` (default: the prover's own
+  // stream); finish() waits for it and serialises KRAK v1.
+  int launch(uint32_t a, uint32_t b, cudaStream_t on = nullptr);
   int finish(uint32_t a, uint32_t b, std::vector<uint8_t>& out);
   bool busy() const;
   uint32_t log_n() const;

@@ -155,13 +155,18 @@ def run_served(engine: Engine, arrivals):
 
 
 def summarize_served(records):
-    by = {}
+    by, wait, run = {}, {}, {}
     for r in records:
         by.setdefault(r["class"], []).append(r["latency_ms"])
+        wait.setdefault(r["class"], []).append((r["t_start"] - r["t_submit"]) * 1e3)
+        run.setdefault(r["class"], []).append((r["t_end"] - r["t_start"]) * 1e3)
     span = max(r["t_end"] for r in records) - min(r["t_submit"] for r in records)
     n_fib = sum(1 for r in records if r["kind"] == FIB)
     return {"jobs": len(records), "seconds": span, "jobs_per_s": len(records) / span, "proofs_per_s": n_fib / span,
             "p50_ms": percentile([r["latency_ms"] for r in records], 0.5),
             "p99_ms": percentile([r["latency_ms"] for r in records], 0.99),
             "per_class": {c: {"n": len(v), "p50_ms": percentile(v, 0.5), "p99_ms": percentile(v, 0.99),
-                              "mean_ms": statistics.mean(v)} for c, v in sorted(by.items())}}
+                              "mean_ms": statistics.mean(v),
+                              "queue_p50_ms": percentile(wait[c], 0.5), "queue_p99_ms": percentile(wait[c], 0.99),
+                              "run_p50_ms": percentile(run[c], 0.5), "run_p99_ms": percentile(run[c], 0.99)}
+                          for c, v in sorted(by.items())}}
