@@ -11,8 +11,16 @@ present, the calls raise.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import re
 from pathlib import Path
+
+# The slot engine keeps up to 24 streams busy (8 slots x 3 priorities); CUDA maps
+# streams onto CUDA_DEVICE_MAX_CONNECTIONS hardware queues (8 by default), and
+# streams that share a queue serialise, so a small job could wait behind a large
+# one. 32 gives each stream its own queue. CUDA reads it when the context is
+# created, so this only takes effect when the package is imported first.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
