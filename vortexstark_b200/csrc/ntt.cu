@@ -225,9 +225,28 @@ __device__ __forceinline__ void rbfly(uint32_t (&v)[32], const TileGeo& g, const
           t[gg + 3] = x << 1;
         }
       } else {
+        // A thread's twiddles of one layer are consecutive and start at a
+        // multiple of their count (hb has zero low bits there), so with aligned
+        // tables they are fetched with 128- or 64-bit loads.
         const uint32_t* tp = tw.layer[g.a + p - C] + hb;
+        const int cnt = K >> (q + 1), o = K - (K >> q);
+        if (tw.vec && cnt >= 4) {
 #pragma unroll
-        for (int gg = 0; gg < (K >> (q + 1)); gg++) t[K - (K >> q) + gg] = __ldg(tp + gg) << 1;
+          for (int v = 0; v < cnt / 4; v++) {
+            const uint4 w = __ldg(reinterpret_cast<const uint4*>(tp) + v);
+            t[o + 4 * v] = w.x << 1;
+            t[o + 4 * v + 1] = w.y << 1;
+            t[o + 4 * v + 2] = w.z << 1;
+            t[o + 4 * v + 3] = w.w << 1;
+          }
+        } else if (tw.vec && cnt == 2) {
+          const uint2 w = __ldg(reinterpret_cast<const uint2*>(tp));
+          t[o] = w.x << 1;
+          t[o + 1] = w.y << 1;
+        } else {
+#pragma unroll
+          for (int gg = 0; gg < cnt; gg++) t[o + gg] = __ldg(tp + gg) << 1;
+        }
       }
     }
 #pragma unroll
@@ -620,11 +639,22 @@ int ntt_lde(const NttColumns& io, uint32_t l, uint32_t B, const NttTw& tw_inv, c
   return VS_OK;
 }
 
+void ntt_tw_check_alignment(NttTw& tw, uint32_t L) {
+  tw.vec = 1;
+  for (uint32_t j = 0; j < L && j < 32; j++) {
+    const uint64_t size = 1ull << (L - 1 - j);                 // entries of layer j
+    const uint64_t need = 4 * (size >= 4 ? 4 : size);          // bytes of alignment a vector load needs
+    const uint32_t* base = (j == 0 && tw.stwo) ? tw.flat : tw.layer[j];
+    if (!base || (reinterpret_cast<uintptr_t>(base) % need) != 0) tw.vec = 0;
+  }
+}
+
 NttTw native_tw(const uint32_t* line, const uint32_t* circle, const uint32_t* offsets, uint32_t n_line_layers) {
   NttTw tw{};
   tw.stwo = 0;
   tw.layer[0] = circle;
   for (uint32_t j = 1; j <= n_line_layers && j < 32; j++) tw.layer[j] = line + offsets[j - 1];
+  ntt_tw_check_alignment(tw, n_line_layers + 1);
   return tw;
 }
 NttTw stwo_tw(const uint32_t* flat, uint32_t L) {
@@ -633,6 +663,7 @@ NttTw stwo_tw(const uint32_t* flat, uint32_t L) {
   tw.flat = flat;
   const uint32_t half = 1u << (L - 1);
   for (uint32_t j = 1; j < L && j < 32; j++) tw.layer[j] = flat + (half - (1u << (L - j)));
+  ntt_tw_check_alignment(tw, L);
   return tw;
 }
 

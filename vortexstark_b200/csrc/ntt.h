@@ -14,7 +14,10 @@ struct NttTw {
   const uint32_t* layer[32];
   const uint32_t* flat;
   int stwo;
+  int vec;  // every layer table is aligned to min(16 B, its size): twiddles may be read with vector loads
 };
+// Sets tw.vec from the table pointers of a transform of 2^log_n points.
+void ntt_tw_check_alignment(NttTw& tw, uint32_t log_n);
 
 struct NttPass {
   const uint32_t* src;

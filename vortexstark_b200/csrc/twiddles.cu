@@ -219,12 +219,15 @@ int get_twiddles(int kind, uint32_t log_n, const TwiddleSet** out, cudaStream_t 
   const unsigned th = 256;
   if (kind == TW_NATIVE) {
     HostCoset c = host_coset(COSET_HALF_COSET, log_n);
-    size_t words = (size_t)(n - 1) * 2 + (size_t)n;  // line, iline, circle, icircle
+    // line, iline, circle, icircle; each table starts on a 16-byte boundary so
+    // the NTT can fetch a thread's consecutive twiddles with 128-bit loads
+    const size_t lp = ((size_t)(n - 1) + 3) & ~(size_t)3, cp = ((size_t)(n / 2) + 3) & ~(size_t)3;
+    size_t words = 2 * lp + 2 * cp;
     if (cudaMalloc(&t->mem, words * 4) != cudaSuccess) { delete t; return set_error(VS_ERR_OOM, "twiddles: alloc"); }
     t->line = t->mem;
-    t->iline = t->line + (n - 1);
-    t->circle = t->iline + (n - 1);
-    t->icircle = t->circle + n / 2;
+    t->iline = t->line + lp;
+    t->circle = t->iline + lp;
+    t->icircle = t->circle + cp;
     native_line_kernel<<<blocks_for(n - 1, th), th, 0, st>>>(c.initial, c.step, log_n, t->line);
     native_circle_kernel<<<blocks_for(n / 2, th), th, 0, st>>>(c.initial, c.step, n / 2, t->circle);
     VS_LAUNCHED("native twiddles");

@@ -16,7 +16,8 @@ struct TwiddleSet {
   int kind = 0;
   uint32_t log_n = 0;
   uint32_t* mem = nullptr;
-  // native: line/iline (n-1 words, reference layout), circle/icircle (n/2)
+  // native: line/iline (n-1 words, reference layout), circle/icircle (n/2),
+  //         each table 16-byte aligned
   // stwo:   line = forward flat table (n/2), iline = inverse flat table (n/2)
   uint32_t* line = nullptr;
   uint32_t* iline = nullptr;
