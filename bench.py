@@ -171,6 +171,63 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- OODS / DEEP quotient kernels
+def oods_quotients(args, V, torch, lde, N, st, ev):
+    """The reference's OODS quotient kernels over the step's LDE: numerators of all
+    columns against one sample (cuda_accumulate_numerators), then the combine of two
+    samples over the evaluation domain (cuda_compute_quotients_combine), as its Cairo
+    prover runs them (cairo_air/prover.rs:2191-2266). Seeded coefficients and
+    domain coordinates; CUDA-event time on the default stream."""
+    L = V.lib()
+    n_cols = lde.shape[0]
+    log_eval = N.bit_length() - 1
+    dev = lambda words: torch.empty(words, dtype=torch.int32, device="cuda")  # noqa: E731
+
+    def seeded(words, seed):
+        t = dev(words)
+        V.check(L.vs_fill_uniform_m31(t.data_ptr(), words, seed, 0, None))
+        return t
+
+    col_ptrs = torch.tensor([lde[c].data_ptr() for c in range(n_cols)], dtype=torch.int64, device="cuda")
+    idx = torch.arange(n_cols, dtype=torch.int32, device="cuda")
+    b, c = seeded(4 * n_cols, SEED + 5), seeded(4 * n_cols, SEED + 6)
+    numer = [dev(N) for _ in range(4)]
+    out = [dev(N) for _ in range(4)]
+    dxs, dys = seeded(N, SEED + 10), seeded(N, SEED + 11)  # stand-in domain coordinates (cost is value-independent)
+    spx, spy, fla = seeded(8, SEED + 7), seeded(8, SEED + 8), seeded(8, SEED + 9)
+    nptr = [torch.tensor([numer[k].data_ptr()] * 2, dtype=torch.int64, device="cuda") for k in range(4)]
+    logs = torch.tensor([log_eval, log_eval], dtype=torch.int32, device="cuda")
+
+    def acc():
+        L.cuda_accumulate_numerators(col_ptrs.data_ptr(), idx.data_ptr(), b.data_ptr(), c.data_ptr(), n_cols, N,
+                                     *[o.data_ptr() for o in numer])
+
+    def comb():
+        L.cuda_compute_quotients_combine(spx.data_ptr(), spy.data_ptr(), fla.data_ptr(), *[x.data_ptr() for x in nptr],
+                                         logs.data_ptr(), 2, dxs.data_ptr(), dys.data_ptr(), log_eval, N,
+                                         *[o.data_ptr() for o in out])
+
+    res = {}
+    hbm = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0)) \
+        if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
+    for name, fn, alg in (("accumulate_numerators", acc, 4 * n_cols * N + 16 * N),
+                          ("quotients_combine", comb, 2 * 16 * N + 8 * N + 16 * N)):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        s0 = torch.cuda.default_stream()
+        e0.record(s0)
+        for _ in range(args.steps):
+            fn()
+        e1.record(s0)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        res[name] = {"ms": ms, "algorithmic_bytes": alg, "achieved_gbs": alg / (ms / 1e3) / 1e9,
+                     "hbm_frac": alg / (ms / 1e3) / 1e9 / hbm}
+    res["workload"] = f"{n_cols} LDE columns x 2^{log_eval} rows; combine of 2 samples"
+    return res
+
+
 # ---------------------------------------------------------------- proof workloads
 def proof_workloads(args):
     """Proof throughput and latency. The plain path is the drop-in single-job
@@ -272,6 +329,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-proofs", action="store_true", help="skip the plain / batched / served proof runs")
+    ap.add_argument("--no-oods", action="store_true", help="skip the OODS quotient kernels")
     ap.add_argument("--slots", type=int, default=8, help="concurrent slots of the batched and served engines")
     ap.add_argument("--served-jobs", type=int, default=600)
     ap.add_argument("--prove-sizes", type=int, nargs="*", default=[20, 24, 28],
@@ -373,6 +431,8 @@ def main():
     three = {"groups": "/".join(str(b - a) for a, b in groups), "ms": m0.elapsed_time(m1) / args.steps,
              "row_packed_root_ms": phase["merkle"]}
 
+    oods = oods_quotients(args, V, torch, lde, N, st, ev) if rank == 0 and not args.no_oods else None
+
     # End to end through the C ABI from pinned host buffers: every step copies its
     # inputs host -> device and reads its roots back. Inputs are double-buffered on
     # the device and copied on a second stream, so step k+1's upload overlaps step
@@ -454,7 +514,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic (seeded SplitMix64 uniform M31)",
                 "config": config_json(args), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": clk.summary(), "three_tree_commit": three,
+                "gpu_launches": launches, "clocks": clk.summary(), "three_tree_commit": three, "oods": oods,
                 "proofs": proofs}
         print(json.dumps(line), flush=True)
     replicas.finalize()

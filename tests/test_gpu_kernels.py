@@ -323,3 +323,42 @@ def test_three_tree_commit_16_15_3(L):
         api.merkle_root_capped(lde[a:b], root)
         torch.cuda.synchronize()
         assert np.array_equal(host(root), O.merkle_root_capped(host(lde[a:b]).reshape(b - a, -1), threads=8))
+
+
+@pytest.mark.parametrize("log_n", [3, 10, 17])
+def test_quotients_combine_zero_denominators(L, log_n):
+    """Rows whose denominator vanishes (domain point equal to the sample point's real
+    parts) get inverse 0, as the reference's per-row Fermat inverse gives; the
+    batched inversion must not let them spoil the other rows of the batch."""
+    rng = np.random.default_rng(20 + log_n)
+    n = 1 << log_n
+    spx, spy, fla = rand_m31(rng, 2, 4), rand_m31(rng, 2, 4), rand_m31(rng, 2, 4)
+    spx[0, 1] = 0
+    spy[0, 1] = 0
+    dxs, dys = rand_m31(rng, n), rand_m31(rng, n)
+    hit = rng.choice(n, size=max(1, n // 7), replace=False)
+    dxs[hit], dys[hit] = spx[0, 0], spy[0, 0]
+    nums = [rand_m31(rng, 4, n), rand_m31(rng, 4, max(2, n // 2))]
+    logs = [log_n, max(1, log_n - 1)]
+    dn = [[dev(x[k]) for k in range(4)] for x in nums]
+    outs = [empty(n) for _ in range(4)]
+    L.cuda_compute_quotients_combine(ptr(dev(spx.reshape(-1))), ptr(dev(spy.reshape(-1))), ptr(dev(fla.reshape(-1))),
+                                     *[ptr(ptr_array([dn[j][k] for j in range(2)])) for k in range(4)],
+                                     ptr(dev(np.array(logs, np.uint32))), 2, ptr(dev(dxs)), ptr(dev(dys)),
+                                     log_n, n, *map(ptr, outs))
+    exp = O.quotients_combine(spx, spy, fla, nums, logs, dxs, dys, log_n)
+    assert np.array_equal(np.stack([host(o) for o in outs]), exp)
+
+
+@pytest.mark.parametrize("n_batch", [1, 34, 300])
+def test_accumulate_numerators_many_columns(L, n_batch):
+    rng = np.random.default_rng(n_batch)
+    n = 3000
+    cols = [rand_m31(rng, n) for _ in range(8)]
+    idx = rng.integers(0, 8, n_batch).astype(np.uint32)
+    b, c = rand_m31(rng, n_batch, 4), rand_m31(rng, n_batch, 4)
+    c[0] = P - 1
+    outs = [empty(n) for _ in range(4)]
+    L.cuda_accumulate_numerators(ptr(ptr_array([dev(x) for x in cols])), ptr(dev(idx)), ptr(dev(b.reshape(-1))),
+                                 ptr(dev(c.reshape(-1))), n_batch, n, *map(ptr, outs))
+    assert np.array_equal(np.stack([host(o) for o in outs]), O.accumulate_numerators(cols, idx, b, c, n))

@@ -62,7 +62,10 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
         objs = list(ex.map(compile_one, sources))
     newest = max(o.stat().st_mtime for o in objs)
     if force or not LIB.exists() or LIB.stat().st_mtime < newest:
-        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", *map(str, objs), "-o", str(LIB)]
+        # --no-undefined: a declaration left without a definition fails the link
+        # instead of producing a library that breaks at load or call time
+        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-Xlinker", "--no-undefined", *map(str, objs),
+               "-o", str(LIB)]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -477,7 +477,7 @@ uint64_t GraphProver::device_bytes() const {
   for (uint32_t l = 0; l < impl->nf; l++) b += (impl->N >> (l + 1)) * 16;
   return b;
 }
-int GraphProver::launch(uint32_t a, uint32_t b) {
+int GraphProver::launch(uint32_t a, uint32_t b, cudaStream_t on) {
   if (a >= h::P || b >= h::P) return set_error(VS_ERR_INVALID, "public inputs must be canonical M31");
   impl->h_ab[0] = a;
   impl->h_ab[1] = b;

@@ -33,29 +33,55 @@ __global__ void interleave_kernel(const uint32_t* __restrict__ e, const uint32_t
   if (i < half_n) *reinterpret_cast<uint2*>(out + 2 * (uint64_t)i) = make_uint2(e[i], o[i]);
 }
 
-// numer[row] = sum_i (c_i * f_i[row] - b_i)   (quotient.cu:25-68)
+// numer[row] = sum_i (c_i * f_i[row] - b_i)   (quotient.cu:25-68), computed as
+// sum_i c_i f_i - sum_i b_i: each product is reduced only to < 2^32 (low 31 bits
+// plus the high part, congruent mod p) and summed per limb in 64 bits, then
+// reduced once; sum_i b_i is formed once per CTA. Same canonical result.
+__device__ __forceinline__ uint64_t mul_lazy(uint32_t x, uint32_t y) {
+  const uint64_t p = (uint64_t)x * y;
+  return (p & VS_P) + (p >> 31);
+}
+__device__ __forceinline__ uint32_t reduce64(uint64_t a) {
+  a = (a & VS_P) + (a >> 31);  // < 2^31 + 2^33
+  a = (a & VS_P) + (a >> 31);  // < 2^31 + 8
+  return canon((uint32_t)a);
+}
 __global__ void accumulate_numerators_kernel(const uint32_t* const* __restrict__ cols, const uint32_t* __restrict__ idx,
                                              const uint32_t* __restrict__ b, const uint32_t* __restrict__ c,
                                              uint32_t n_batch, uint32_t n_rows, uint32_t* __restrict__ o0,
                                              uint32_t* __restrict__ o1, uint32_t* __restrict__ o2,
                                              uint32_t* __restrict__ o3) {
-  uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= n_rows) return;
-  qm31 acc = qzero();
-  for (uint32_t k = 0; k < n_batch; k++) {
-    uint32_t f = cols[idx[k]][row];
-    qm31 ck{{__ldg(c + 4 * k), __ldg(c + 4 * k + 1), __ldg(c + 4 * k + 2), __ldg(c + 4 * k + 3)}};
-    qm31 bk{{__ldg(b + 4 * k), __ldg(b + 4 * k + 1), __ldg(b + 4 * k + 2), __ldg(b + 4 * k + 3)}};
-    acc = qadd(acc, qsub(qscale(ck, f), bk));
+  __shared__ uint32_t bsum[4];
+  if (threadIdx.x < 4) {
+    uint32_t acc = 0;
+    for (uint32_t k = 0; k < n_batch; k++) acc = add(acc, __ldg(b + 4 * k + threadIdx.x));
+    bsum[threadIdx.x] = acc;
   }
-  o0[row] = acc.v[0];
-  o1[row] = acc.v[1];
-  o2[row] = acc.v[2];
-  o3[row] = acc.v[3];
+  __syncthreads();
+  const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n_rows) return;
+  uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  for (uint32_t k = 0; k < n_batch; k++) {
+    const uint32_t f = cols[idx[k]][row];
+    a0 += mul_lazy(__ldg(c + 4 * k), f);  // scalar loads: c carries no alignment promise
+    a1 += mul_lazy(__ldg(c + 4 * k + 1), f);
+    a2 += mul_lazy(__ldg(c + 4 * k + 2), f);
+    a3 += mul_lazy(__ldg(c + 4 * k + 3), f);
+  }
+  o0[row] = sub(reduce64(a0), bsum[0]);
+  o1[row] = sub(reduce64(a1), bsum[1]);
+  o2[row] = sub(reduce64(a2), bsum[2]);
+  o3[row] = sub(reduce64(a3), bsum[3]);
 }
 
 // q[row] = sum_j (numer_j[lift(row)] - A_j * y) * D_j(row)^-1 with
-// D = (Re sx - x) Im sy - (Re sy - y) Im sx in CM31   (quotient.cu:101-197)
+// D = (Re sx - x) Im sy - (Re sy - y) Im sx in CM31   (quotient.cu:101-197).
+// The reference inverts every D with a Fermat power; here each thread takes
+// QC_ROWS rows (strided by the grid for coalescing) and inverts their D_j with
+// one inverse and a Montgomery product chain. A zero D is left out of the chain
+// and gets inverse 0, as the Fermat power gives, so results are identical.
+constexpr int QC_ROWS = 8;
+__device__ __forceinline__ bool czero(cm31 x) { return (x.a | x.b) == 0; }
 __global__ void quotients_combine_kernel(const uint32_t* __restrict__ spx, const uint32_t* __restrict__ spy,
                                          const uint32_t* __restrict__ fla, const uint32_t* const* __restrict__ n0,
                                          const uint32_t* const* __restrict__ n1, const uint32_t* const* __restrict__ n2,
@@ -64,25 +90,56 @@ __global__ void quotients_combine_kernel(const uint32_t* __restrict__ spx, const
                                          const uint32_t* __restrict__ dys, uint32_t lifting_log, uint32_t n_rows,
                                          uint32_t* __restrict__ o0, uint32_t* __restrict__ o1,
                                          uint32_t* __restrict__ o2, uint32_t* __restrict__ o3) {
-  uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= n_rows) return;
-  const uint32_t dx = dxs[row], dy = dys[row];
-  qm31 q = qzero();
-  for (uint32_t j = 0; j < n_accs; j++) {
-    cm31 prx{spx[4 * j], spx[4 * j + 1]}, pix{spx[4 * j + 2], spx[4 * j + 3]};
-    cm31 pry{spy[4 * j], spy[4 * j + 1]}, piy{spy[4 * j + 2], spy[4 * j + 3]};
-    cm31 den = csub(cmul(csub(prx, cm31{dx, 0}), piy), cmul(csub(pry, cm31{dy, 0}), pix));
-    cm31 di = cinv(den);
-    uint32_t ratio = lifting_log - acc_log[j];
-    uint32_t li = ((row >> (ratio + 1)) << 1) + (row & 1);
-    qm31 pn{{n0[j][li], n1[j][li], n2[j][li], n3[j][li]}};
-    qm31 a{{fla[4 * j], fla[4 * j + 1], fla[4 * j + 2], fla[4 * j + 3]}};
-    q = qadd(q, qscale_c(qsub(pn, qscale(a, dy)), di));
+  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t dx[QC_ROWS], dy[QC_ROWS];
+  qm31 q[QC_ROWS];
+#pragma unroll
+  for (int i = 0; i < QC_ROWS; i++) {
+    const uint32_t row = t0 + i * stride;
+    const bool live = row < n_rows;
+    dx[i] = live ? dxs[row] : 0u;
+    dy[i] = live ? dys[row] : 0u;
+    q[i] = qzero();
   }
-  o0[row] = q.v[0];
-  o1[row] = q.v[1];
-  o2[row] = q.v[2];
-  o3[row] = q.v[3];
+  for (uint32_t j = 0; j < n_accs; j++) {
+    const cm31 prx{spx[4 * j], spx[4 * j + 1]}, pix{spx[4 * j + 2], spx[4 * j + 3]};
+    const cm31 pry{spy[4 * j], spy[4 * j + 1]}, piy{spy[4 * j + 2], spy[4 * j + 3]};
+    const qm31 a{{fla[4 * j], fla[4 * j + 1], fla[4 * j + 2], fla[4 * j + 3]}};
+    const uint32_t ratio = lifting_log - acc_log[j];
+    const uint32_t *p0 = n0[j], *p1 = n1[j], *p2 = n2[j], *p3 = n3[j];
+    cm31 den[QC_ROWS], pre[QC_ROWS];
+    cm31 run{1, 0};
+#pragma unroll
+    for (int i = 0; i < QC_ROWS; i++) {
+      den[i] = csub(cmul(csub(prx, cm31{dx[i], 0}), piy), cmul(csub(pry, cm31{dy[i], 0}), pix));
+      pre[i] = run;
+      if (!czero(den[i])) run = cmul(run, den[i]);
+    }
+    cm31 inv = cinv(run);  // run is never zero
+#pragma unroll
+    for (int i = QC_ROWS - 1; i >= 0; i--) {
+      const bool z = czero(den[i]);
+      const cm31 di = z ? cm31{0, 0} : cmul(inv, pre[i]);
+      if (!z) inv = cmul(inv, den[i]);
+      const uint32_t row = t0 + i * stride;
+      if (row < n_rows) {
+        const uint32_t li = ((row >> (ratio + 1)) << 1) + (row & 1);
+        const qm31 pn{{p0[li], p1[li], p2[li], p3[li]}};
+        q[i] = qadd(q[i], qscale_c(qsub(pn, qscale(a, dy[i])), di));
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < QC_ROWS; i++) {
+    const uint32_t row = t0 + i * stride;
+    if (row < n_rows) {
+      o0[row] = q[i].v[0];
+      o1[row] = q[i].v[1];
+      o2[row] = q[i].v[2];
+      o3[row] = q[i].v[3];
+    }
+  }
 }
 
 __global__ void m31_binop_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
@@ -157,8 +214,8 @@ void cuda_compute_quotients_combine(const uint32_t* spx, const uint32_t* spy, co
                                     const uint32_t* dxs, const uint32_t* dys, uint32_t lifting_log, uint32_t n_rows,
                                     uint32_t* o0, uint32_t* o1, uint32_t* o2, uint32_t* o3) {
   if (!n_rows) return;
-  quotients_combine_kernel<<<blocks_for(n_rows, 256), 256>>>(spx, spy, fla, n0, n1, n2, n3, acc_log, n_accs, dxs, dys,
-                                                             lifting_log, n_rows, o0, o1, o2, o3);
+  quotients_combine_kernel<<<blocks_for((n_rows + QC_ROWS - 1) / QC_ROWS, 256), 256>>>(
+      spx, spy, fla, n0, n1, n2, n3, acc_log, n_accs, dxs, dys, lifting_log, n_rows, o0, o1, o2, o3);
   check_cuda(cudaGetLastError(), "cuda_compute_quotients_combine");
 }
 void cuda_m31_add(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n) {
