@@ -350,15 +350,20 @@ def test_quotients_combine_zero_denominators(L, log_n):
     assert np.array_equal(np.stack([host(o) for o in outs]), exp)
 
 
-@pytest.mark.parametrize("n_batch", [1, 34, 300])
-def test_accumulate_numerators_many_columns(L, n_batch):
-    rng = np.random.default_rng(n_batch)
-    n = 3000
+@pytest.mark.parametrize("n_batch,n,shift", [(1, 3000, 0), (34, 3000, 0), (300, 3000, 0), (34, 3001, 0),
+                                              (7, 1027, 1), (34, 4096, 3)])
+def test_accumulate_numerators_many_columns(L, n_batch, n, shift):
+    """Column counts past the 3-term fold period, ragged row counts and columns /
+    outputs that start off a 16-byte boundary (the 128-bit paths fall back)."""
+    rng = np.random.default_rng(n_batch + n)
     cols = [rand_m31(rng, n) for _ in range(8)]
     idx = rng.integers(0, 8, n_batch).astype(np.uint32)
     b, c = rand_m31(rng, n_batch, 4), rand_m31(rng, n_batch, 4)
     c[0] = P - 1
-    outs = [empty(n) for _ in range(4)]
-    L.cuda_accumulate_numerators(ptr(ptr_array([dev(x) for x in cols])), ptr(dev(idx)), ptr(dev(b.reshape(-1))),
-                                 ptr(dev(c.reshape(-1))), n_batch, n, *map(ptr, outs))
-    assert np.array_equal(np.stack([host(o) for o in outs]), O.accumulate_numerators(cols, idx, b, c, n))
+    dcols = [dev(np.concatenate([np.zeros(shift, np.uint32), x])) for x in cols]
+    col_ptrs = ptr_array([d[shift:] for d in dcols])
+    outs = [empty(n + shift) for _ in range(4)]
+    L.cuda_accumulate_numerators(ptr(col_ptrs), ptr(dev(idx)), ptr(dev(b.reshape(-1))), ptr(dev(c.reshape(-1))),
+                                 n_batch, n, *[ptr(o[shift:]) for o in outs])
+    got = np.stack([host(o)[shift:] for o in outs])
+    assert np.array_equal(got, O.accumulate_numerators(cols, idx, b, c, n))
