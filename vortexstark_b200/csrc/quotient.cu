@@ -36,7 +36,8 @@ __global__ void interleave_kernel(const uint32_t* __restrict__ e, const uint32_t
 // numer[row] = sum_i (c_i * f_i[row] - b_i)   (quotient.cu:25-68), computed as
 // sum_i c_i f_i - sum_i b_i. Products c_i * f_i (< 2^62) are accumulated per limb
 // with 64-bit multiply-adds; every three terms the sum is folded to < 2^34
-// (2^31 == 1 mod p), so it never overflows, and it is reduced once at the end.
+// (2^31 == 1 mod p), so it never overflows (a fold leaves < 2^34, plus at most
+// three products < 2^62 each), and it is reduced once at the end.
 // sum_i b_i is formed once per CTA. Each thread takes 4 consecutive rows, read
 // with one 128-bit load per column where the column is 16-byte aligned. Same
 // canonical result as the term-by-term reference.
@@ -66,10 +67,10 @@ __global__ void accumulate_numerators_kernel(const uint32_t* const* __restrict__
   for (int r = 0; r < AN_ROWS; r++)
 #pragma unroll
     for (int l = 0; l < 4; l++) acc[r][l] = 0;
-  uint32_t since_fold = 0;
-  for (uint32_t k = 0; k < n_batch; k++) {
+  // Columns go in groups of three (the fold period): the group's loads are all
+  // issued before its multiply-adds, so three HBM reads are in flight per thread.
+  auto load = [&](uint32_t k, uint32_t (&f)[AN_ROWS]) {
     const uint32_t* col = cols[idx[k]];
-    uint32_t f[AN_ROWS];
     if (full && (reinterpret_cast<uintptr_t>(col + row0) & 15) == 0) {
       const uint4 v = __ldg(reinterpret_cast<const uint4*>(col + row0));
       f[0] = v.x; f[1] = v.y; f[2] = v.z; f[3] = v.w;
@@ -77,18 +78,35 @@ __global__ void accumulate_numerators_kernel(const uint32_t* const* __restrict__
 #pragma unroll
       for (int r = 0; r < AN_ROWS; r++) f[r] = row0 + r < n_rows ? col[row0 + r] : 0u;
     }
+  };
+  auto mac = [&](uint32_t k, const uint32_t (&f)[AN_ROWS]) {
     const uint32_t cl[4] = {__ldg(c + 4 * k), __ldg(c + 4 * k + 1), __ldg(c + 4 * k + 2), __ldg(c + 4 * k + 3)};
 #pragma unroll
     for (int r = 0; r < AN_ROWS; r++)
 #pragma unroll
       for (int l = 0; l < 4; l++) acc[r][l] += (uint64_t)cl[l] * f[r];
-    if (++since_fold == 3) {
-      since_fold = 0;
+  };
+  auto fold_all = [&]() {
 #pragma unroll
-      for (int r = 0; r < AN_ROWS; r++)
+    for (int r = 0; r < AN_ROWS; r++)
 #pragma unroll
-        for (int l = 0; l < 4; l++) acc[r][l] = fold31(acc[r][l]);
-    }
+      for (int l = 0; l < 4; l++) acc[r][l] = fold31(acc[r][l]);
+  };
+  uint32_t k = 0;
+  for (; k + 3 <= n_batch; k += 3) {
+    uint32_t f0[AN_ROWS], f1[AN_ROWS], f2[AN_ROWS];
+    load(k, f0);
+    load(k + 1, f1);
+    load(k + 2, f2);
+    mac(k, f0);
+    mac(k + 1, f1);
+    mac(k + 2, f2);
+    fold_all();
+  }
+  for (; k < n_batch; k++) {  // at most two: no fold needed before the final reduction
+    uint32_t f0[AN_ROWS];
+    load(k, f0);
+    mac(k, f0);
   }
   uint32_t* out[4] = {o0, o1, o2, o3};
 #pragma unroll
@@ -112,7 +130,7 @@ __global__ void accumulate_numerators_kernel(const uint32_t* const* __restrict__
 // QC_ROWS rows (strided by the grid for coalescing) and inverts their D_j with
 // one inverse and a Montgomery product chain. A zero D is left out of the chain
 // and gets inverse 0, as the Fermat power gives, so results are identical.
-constexpr int QC_ROWS = 8;
+constexpr int QC_ROWS = 4;
 __device__ __forceinline__ bool czero(cm31 x) { return (x.a | x.b) == 0; }
 __global__ void quotients_combine_kernel(const uint32_t* __restrict__ spx, const uint32_t* __restrict__ spy,
                                          const uint32_t* __restrict__ fla, const uint32_t* const* __restrict__ n0,
