@@ -242,7 +242,9 @@ def proof_workloads(args):
             eng.prepare(api.commit_job(j.log_n, 34, 0) if j.kind == api.COMMIT else j)
 
     out = {}
-    api.init_memory_pool(2 << 30)  # as the reference's prover initialises its pool
+    # the stream-ordered pool keeps what it has allocated, as the reference's own
+    # benchmark sets it (init_memory_pool_greedy, src/bin/full_benchmark.rs:23)
+    api.init_memory_pool((1 << 64) - 1)
     plain = W.plain_jobs(64, 16)
     W.run_plain(plain[:4])
     t_plain, r_plain = W.run_plain(plain)
