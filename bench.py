@@ -496,12 +496,19 @@ def main():
     # all phases are integer-ALU bound (Blake2s, M31 butterflies), not HBM bound.
     hbm = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0)) \
         if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
+    clk_hz = (clk.summary()["sm_mhz"] or 1965.0) * 1e6
     alg = {"lde": n_cols * (4 * n + 4 * N), "merkle": n_cols * 4 * N,
            "fri": sum(24 * (1 << (l - 1)) for l in range(4, fri_log + 1))}
     ach = alg["merkle"] / (phase["merkle"] / 1e3) / 1e9
     roof = {"bound": "hbm", "kernel": "merkle_subtree_kernel<LeafRowPacked>", "achieved": ach, "peak": hbm,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)", "unit": "GB/s", "frac": ach / hbm,
             "traffic": alg["merkle"] * 1.0004, "algorithmic_bytes": alg["merkle"],
+            # The binding resource is integer issue: instructions per launch (1286
+            # per Blake2s compression, the ncu count of this kernel; one
+            # compression per 64 B of leaf plus one per node) over 148 SMs x 4
+            # schedulers x 32 lanes x the sampled SM clock.
+            "int_issue_frac": (-(-n_cols * 4 // 64) + 1) * 1286 * N / (phase["merkle"] / 1e3)
+                              / (148 * 4 * 32 * clk_hz),
             "launch_ms": phase["merkle"], "phase_ms": phase,
             "phase_hbm_frac": {k: alg[k] / (phase[k] / 1e3) / 1e9 / hbm for k in phase}}
 
