@@ -4,6 +4,7 @@
 
 #include "vs_blake2s.cuh"
 #include "vs_field.cuh"
+#include "vs_mem.cuh"
 
 namespace vs {
 
@@ -34,10 +35,10 @@ struct LeafFold {
   qm31 alpha, alpha_sq;
   int accumulate;
   __device__ __forceinline__ void operator()(uint64_t i, uint32_t out[8]) const {
-    uint2 a0 = *reinterpret_cast<const uint2*>(src.c[0] + 2 * i);
-    uint2 a1 = *reinterpret_cast<const uint2*>(src.c[1] + 2 * i);
-    uint2 a2 = *reinterpret_cast<const uint2*>(src.c[2] + 2 * i);
-    uint2 a3 = *reinterpret_cast<const uint2*>(src.c[3] + 2 * i);
+    uint2 a0 = ld2(src.c[0] + 2 * i);
+    uint2 a1 = ld2(src.c[1] + 2 * i);
+    uint2 a2 = ld2(src.c[2] + 2 * i);
+    uint2 a3 = ld2(src.c[3] + 2 * i);
     qm31 f0{{a0.x, a1.x, a2.x, a3.x}}, f1{{a0.y, a1.y, a2.y, a3.y}};
     qm31 r = fold_pair(f0, f1, alpha, __ldg(tw + i));
     if (accumulate) {

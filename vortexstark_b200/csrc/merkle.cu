@@ -2,6 +2,7 @@
 // cuda/merkle_leaves_lifted.cu, and vs_merkle_root_* (root-only commitments).
 #include "merkle.h"
 #include "vs_field.cuh"
+#include "vs_mem.cuh"
 
 namespace vs {
 
@@ -11,23 +12,21 @@ __global__ void leaf_hash_kernel(Leaf leaf, uint64_t n, uint32_t* __restrict__ o
   if (i >= n) return;
   uint32_t h[8];
   leaf(i, h);
-  uint4* o = reinterpret_cast<uint4*>(out + 8 * i);
-  o[0] = make_uint4(h[0], h[1], h[2], h[3]);
-  o[1] = make_uint4(h[4], h[5], h[6], h[7]);
+  st4(out + 8 * i, make_uint4(h[0], h[1], h[2], h[3]));
+  st4(out + 8 * i + 4, make_uint4(h[4], h[5], h[6], h[7]));
 }
 
 __global__ void hash_nodes_kernel(const uint32_t* __restrict__ children, uint32_t* __restrict__ parents, uint64_t n) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint4* c = reinterpret_cast<const uint4*>(children + 16 * i);
-  uint4 a = c[0], b = c[1], d = c[2], e = c[3];
+  const uint32_t* c = children + 16 * i;
+  const uint4 a = ld4_ro(c), b = ld4_ro(c + 4), d = ld4_ro(c + 8), e = ld4_ro(c + 12);
   uint32_t m[16] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, d.x, d.y, d.z, d.w, e.x, e.y, e.z, e.w};
   uint32_t h[8];
   b2s_init(h);
   b2s_compress(h, m, 64u, true);
-  uint4* o = reinterpret_cast<uint4*>(parents + 8 * i);
-  o[0] = make_uint4(h[0], h[1], h[2], h[3]);
-  o[1] = make_uint4(h[4], h[5], h[6], h[7]);
+  st4(parents + 8 * i, make_uint4(h[0], h[1], h[2], h[3]));
+  st4(parents + 8 * i + 4, make_uint4(h[4], h[5], h[6], h[7]));
 }
 
 // Parent of each SoA4 leaf pair (blake2s.cu:190-231 semantics).

@@ -15,6 +15,7 @@
 #include <cstdint>
 
 #include "vs_blake2s.cuh"
+#include "vs_mem.cuh"
 
 namespace vs {
 
@@ -76,8 +77,7 @@ __global__ void __launch_bounds__(MK_THREADS) merkle_subtree_kernel(Leaf leaf, u
 struct LeafHashes {
   const uint32_t* h;
   __device__ __forceinline__ void operator()(uint64_t i, uint32_t out[8]) const {
-    const uint4* p = reinterpret_cast<const uint4*>(h + 8 * i);
-    uint4 a = p[0], b = p[1];
+    const uint4 a = ld4_ro(h + 8 * i), b = ld4_ro(h + 8 * i + 4);
     out[0] = a.x; out[1] = a.y; out[2] = a.z; out[3] = a.w;
     out[4] = b.x; out[5] = b.y; out[6] = b.z; out[7] = b.w;
   }

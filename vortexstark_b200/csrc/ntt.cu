@@ -226,11 +226,12 @@ __device__ __forceinline__ void rbfly(uint32_t (&v)[32], const TileGeo& g, const
         }
       } else {
         // A thread's twiddles of one layer are consecutive and start at a
-        // multiple of their count (hb has zero low bits there), so with aligned
-        // tables they are fetched with 128- or 64-bit loads.
+        // multiple of their count (hb has zero low bits there); the host side
+        // hands the kernels tables aligned to min(16 B, table size), so they are
+        // fetched with 128- or 64-bit loads.
         const uint32_t* tp = tw.layer[g.a + p - C] + hb;
         const int cnt = K >> (q + 1), o = K - (K >> q);
-        if (tw.vec && cnt >= 4) {
+        if (cnt >= 4) {
 #pragma unroll
           for (int v = 0; v < cnt / 4; v++) {
             const uint4 w = __ldg(reinterpret_cast<const uint4*>(tp) + v);
@@ -239,7 +240,7 @@ __device__ __forceinline__ void rbfly(uint32_t (&v)[32], const TileGeo& g, const
             t[o + 4 * v + 2] = w.z << 1;
             t[o + 4 * v + 3] = w.w << 1;
           }
-        } else if (tw.vec && cnt == 2) {
+        } else if (cnt == 2) {
           const uint2 w = __ldg(reinterpret_cast<const uint2*>(tp));
           t[o] = w.x << 1;
           t[o + 1] = w.y << 1;
@@ -539,7 +540,110 @@ static int small_transform(uint32_t* d, uint32_t L, const NttTw& tw, bool fwd, u
   return VS_OK;
 }
 
+// ------------------------------------------------------------------ alignment
+// The pass and LDE kernels move 16-byte chunks (cp.async, 128-bit loads and
+// stores) and read twiddles with 64/128-bit loads. Entry points accept any
+// 4-byte-aligned device pointer, as the reference's word-by-word kernels do, so
+// the host side checks column starts, strides and twiddle tables first and, when
+// one is not aligned, runs the transform on aligned copies (stream-ordered
+// temporaries) instead. The kernels themselves never see an unaligned address.
+namespace {
+bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Stream-ordered temporaries released on the stream when the scope ends.
+struct StreamScratch {
+  cudaStream_t st;
+  std::vector<void*> ptrs;
+  explicit StreamScratch(cudaStream_t s) : st(s) {}
+  ~StreamScratch() {
+    for (void* p : ptrs) cudaFreeAsync(p, st);
+  }
+  int alloc(uint32_t** out, uint64_t words) {
+    VS_CUDA(cudaMallocAsync((void**)out, std::max<uint64_t>(words, 4) * 4, st));
+    ptrs.push_back(*out);
+    return VS_OK;
+  }
+};
+
+// Twiddles the kernels can read with vector loads: tw itself when its tables
+// are aligned, else copies of the read part of every layer at aligned offsets.
+int aligned_twiddles(const NttTw& tw, uint32_t L, cudaStream_t st, StreamScratch& tmp, NttTw* out) {
+  if (tw.vec) { *out = tw; return VS_OK; }
+  if (tw.stwo) {
+    uint32_t* f = nullptr;
+    const uint64_t words = 1ull << (L - 1);  // the flat table: pairs of the circle layer and all line layers
+    VS_TRY(tmp.alloc(&f, words));
+    VS_CUDA(cudaMemcpyAsync(f, tw.flat, words * 4, cudaMemcpyDeviceToDevice, st));
+    *out = stwo_tw(f, L);
+  } else {
+    uint64_t off[32] = {0}, total = 0;
+    for (uint32_t j = 0; j < L && j < 32; j++) {
+      off[j] = total;
+      total += ((1ull << (L - 1 - j)) + 3) & ~3ull;  // layer j reads 2^(L-1-j) twiddles
+    }
+    uint32_t* base = nullptr;
+    VS_TRY(tmp.alloc(&base, total));
+    NttTw t{};
+    t.stwo = 0;
+    for (uint32_t j = 0; j < L && j < 32; j++) {
+      VS_CUDA(cudaMemcpyAsync(base + off[j], tw.layer[j], (1ull << (L - 1 - j)) * 4, cudaMemcpyDeviceToDevice, st));
+      t.layer[j] = base + off[j];
+    }
+    ntt_tw_check_alignment(t, L);
+    *out = t;
+  }
+  if (!out->vec) return set_error(VS_ERR_INVALID, "ntt: twiddle staging left a table unaligned");
+  return VS_OK;
+}
+
+// Host copies of the column pointers and whether every column start (and stride)
+// is 16-byte aligned. Pointer arrays are read back from the device (the batched
+// entry points that pass them synchronise anyway).
+int column_pointers(const NttColumns& io, std::vector<const uint32_t*>& src, std::vector<uint32_t*>& dst, bool* ok) {
+  src.resize(io.n_cols);
+  dst.resize(io.n_cols);
+  if (io.src_cols) VS_CUDA(cudaMemcpy(src.data(), io.src_cols, io.n_cols * sizeof(void*), cudaMemcpyDeviceToHost));
+  else for (uint32_t c = 0; c < io.n_cols; c++) src[c] = io.src + c * io.src_stride;
+  if (io.dst_cols) VS_CUDA(cudaMemcpy(dst.data(), io.dst_cols, io.n_cols * sizeof(void*), cudaMemcpyDeviceToHost));
+  else for (uint32_t c = 0; c < io.n_cols; c++) dst[c] = io.dst + c * io.dst_stride;
+  *ok = true;
+  for (uint32_t c = 0; c < io.n_cols; c++) *ok = *ok && al16(src[c]) && al16(dst[c]);
+  return VS_OK;
+}
+bool strided_aligned(const NttColumns& io) {
+  if (io.src_cols || io.dst_cols) return false;  // decided from the pointer values
+  const bool multi = io.n_cols > 1;
+  return al16(io.src) && al16(io.dst) && (!multi || (io.src_stride % 4 == 0 && io.dst_stride % 4 == 0));
+}
+}  // namespace
+
+static int ntt_transform_aligned(const NttColumns& io, uint32_t L, const NttTw& tw, bool fwd, cudaStream_t st);
+
 int ntt_transform(const NttColumns& io, uint32_t L, const NttTw& tw, bool fwd, cudaStream_t st) {
+  if (L == 0) return VS_OK;
+  if (L < 5) return ntt_transform_aligned(io, L, tw, fwd, st);  // word-by-word kernels
+  StreamScratch tmp(st);
+  NttTw t;
+  VS_TRY(aligned_twiddles(tw, L, st, tmp, &t));
+  if (strided_aligned(io)) return ntt_transform_aligned(io, L, t, fwd, st);
+  std::vector<const uint32_t*> src;
+  std::vector<uint32_t*> dst;
+  bool ok = false;
+  VS_TRY(column_pointers(io, src, dst, &ok));
+  if (ok) return ntt_transform_aligned(io, L, t, fwd, st);
+  const uint64_t n = 1ull << L;
+  uint32_t* T = nullptr;
+  VS_TRY(tmp.alloc(&T, n * io.n_cols));
+  for (uint32_t c = 0; c < io.n_cols; c++)
+    VS_CUDA(cudaMemcpyAsync(T + c * n, src[c], n * 4, cudaMemcpyDeviceToDevice, st));
+  NttColumns tio{T, T, nullptr, nullptr, n, n, io.n_cols};
+  VS_TRY(ntt_transform_aligned(tio, L, t, fwd, st));
+  for (uint32_t c = 0; c < io.n_cols; c++)
+    VS_CUDA(cudaMemcpyAsync(dst[c], T + c * n, n * 4, cudaMemcpyDeviceToDevice, st));
+  return VS_OK;
+}
+
+static int ntt_transform_aligned(const NttColumns& io, uint32_t L, const NttTw& tw, bool fwd, cudaStream_t st) {
   if (L == 0) return VS_OK;
   if (L < 5) {
     for (uint32_t c = 0; c < io.n_cols; c++) {
@@ -574,10 +678,33 @@ int ntt_transform(const NttColumns& io, uint32_t L, const NttTw& tw, bool fwd, c
   return VS_OK;
 }
 
+static int ntt_lde_aligned(const NttColumns& io, uint32_t l, uint32_t B, const NttTw& tw_inv, const NttTw& tw_fwd,
+                           cudaStream_t st);
+
 int ntt_lde(const NttColumns& io, uint32_t l, uint32_t B, const NttTw& tw_inv, const NttTw& tw_fwd,
             cudaStream_t st) {
   if (l < 5) return set_error(VS_ERR_INVALID, "LDE needs log_n >= 5 (got %u)", l);
   if (io.src_cols || io.dst_cols) return set_error(VS_ERR_INVALID, "LDE takes strided columns");
+  StreamScratch tmp(st);
+  NttTw ti, tf;
+  VS_TRY(aligned_twiddles(tw_inv, l, st, tmp, &ti));
+  VS_TRY(aligned_twiddles(tw_fwd, l + B, st, tmp, &tf));
+  if (strided_aligned(io)) return ntt_lde_aligned(io, l, B, ti, tf, st);
+  const uint64_t n = 1ull << l, N = n << B;
+  uint32_t *S = nullptr, *D = nullptr;
+  VS_TRY(tmp.alloc(&S, n * io.n_cols));
+  VS_TRY(tmp.alloc(&D, N * io.n_cols));
+  for (uint32_t c = 0; c < io.n_cols; c++)
+    VS_CUDA(cudaMemcpyAsync(S + c * n, io.src + c * io.src_stride, n * 4, cudaMemcpyDeviceToDevice, st));
+  NttColumns tio{S, D, nullptr, nullptr, n, N, io.n_cols};
+  VS_TRY(ntt_lde_aligned(tio, l, B, ti, tf, st));
+  for (uint32_t c = 0; c < io.n_cols; c++)
+    VS_CUDA(cudaMemcpyAsync(io.dst + c * io.dst_stride, D + c * N, N * 4, cudaMemcpyDeviceToDevice, st));
+  return VS_OK;
+}
+
+static int ntt_lde_aligned(const NttColumns& io, uint32_t l, uint32_t B, const NttTw& tw_inv, const NttTw& tw_fwd,
+                           cudaStream_t st) {
   auto passes = plan_passes(l);
   const size_t np = passes.size();
   // 1. inverse passes below the top one: src -> dst[0, n)

@@ -1,7 +1,11 @@
 // Constraint and OODS quotient kernels: drop-in for cuda/constraint.cu and
 // cuda/quotient.cu, plus the elementwise helpers of cuda/fields.cu.
+#include <algorithm>
+#include <vector>
+
 #include "vs_common.cuh"
 #include "vs_field.cuh"
+#include "vs_mem.cuh"
 
 namespace vs {
 
@@ -30,23 +34,27 @@ __global__ void zero_pad_kernel(const uint32_t* __restrict__ src, uint32_t* __re
 __global__ void interleave_kernel(const uint32_t* __restrict__ e, const uint32_t* __restrict__ o,
                                   uint32_t* __restrict__ out, uint32_t half_n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < half_n) *reinterpret_cast<uint2*>(out + 2 * (uint64_t)i) = make_uint2(e[i], o[i]);
+  if (i < half_n) st2(out + 2 * (uint64_t)i, make_uint2(e[i], o[i]));
 }
 
 // numer[row] = sum_i (c_i * f_i[row] - b_i)   (quotient.cu:25-68), computed as
 // sum_i c_i f_i - sum_i b_i. Products c_i * f_i (< 2^62) are accumulated per limb
 // with 64-bit multiply-adds; every three terms the sum is folded to < 2^34
 // (2^31 == 1 mod p), so it never overflows (a fold leaves < 2^34, plus at most
-// three products < 2^62 each), and it is reduced once at the end.
-// sum_i b_i is formed once per CTA. Each thread takes 4 consecutive rows, read
-// with one 128-bit load per column where the column is 16-byte aligned. Same
-// canonical result as the term-by-term reference.
+// three products < 2^62 each), and it is reduced once at the end. sum_i b_i is
+// formed once per CTA. Each thread takes AN_ROWS rows and a three-column group
+// keeps 3 loads per row in flight. VEC: the rows are consecutive and read and
+// written with 128-bit accesses (the host has checked that every column, output
+// and the row count allow it); otherwise the rows are strided by the grid and
+// every access is a coalesced word. Same canonical result as the term-by-term
+// reference.
 constexpr int AN_ROWS = 4;
 __device__ __forceinline__ uint64_t fold31(uint64_t a) { return (a & VS_P) + (a >> 31); }
 __device__ __forceinline__ uint32_t reduce64(uint64_t a) {
   a = fold31(fold31(a));  // < 2^31 + 8
   return canon((uint32_t)a);
 }
+template <bool VEC>
 __global__ void accumulate_numerators_kernel(const uint32_t* const* __restrict__ cols, const uint32_t* __restrict__ idx,
                                              const uint32_t* __restrict__ b, const uint32_t* __restrict__ c,
                                              uint32_t n_batch, uint32_t n_rows, uint32_t* __restrict__ o0,
@@ -59,24 +67,26 @@ __global__ void accumulate_numerators_kernel(const uint32_t* const* __restrict__
     bsum[threadIdx.x] = acc;
   }
   __syncthreads();
-  const uint32_t row0 = (blockIdx.x * blockDim.x + threadIdx.x) * AN_ROWS;
-  if (row0 >= n_rows) return;
-  const bool full = row0 + AN_ROWS <= n_rows;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t stride = VEC ? 1u : gridDim.x * blockDim.x;   // between a thread's rows
+  const uint32_t t0 = VEC ? tid * AN_ROWS : tid;
+  if (t0 >= n_rows) return;
   uint64_t acc[AN_ROWS][4];
 #pragma unroll
   for (int r = 0; r < AN_ROWS; r++)
 #pragma unroll
     for (int l = 0; l < 4; l++) acc[r][l] = 0;
-  // Columns go in groups of three (the fold period): the group's loads are all
-  // issued before its multiply-adds, so three HBM reads are in flight per thread.
   auto load = [&](uint32_t k, uint32_t (&f)[AN_ROWS]) {
     const uint32_t* col = cols[idx[k]];
-    if (full && (reinterpret_cast<uintptr_t>(col + row0) & 15) == 0) {
-      const uint4 v = __ldg(reinterpret_cast<const uint4*>(col + row0));
+    if (VEC) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(col + t0));
       f[0] = v.x; f[1] = v.y; f[2] = v.z; f[3] = v.w;
     } else {
 #pragma unroll
-      for (int r = 0; r < AN_ROWS; r++) f[r] = row0 + r < n_rows ? col[row0 + r] : 0u;
+      for (int r = 0; r < AN_ROWS; r++) {
+        const uint32_t row = t0 + r * stride;
+        f[r] = row < n_rows ? __ldg(col + row) : 0u;
+      }
     }
   };
   auto mac = [&](uint32_t k, const uint32_t (&f)[AN_ROWS]) {
@@ -109,17 +119,20 @@ __global__ void accumulate_numerators_kernel(const uint32_t* const* __restrict__
     mac(k, f0);
   }
   uint32_t* out[4] = {o0, o1, o2, o3};
+  if (VEC) {
 #pragma unroll
-  for (int l = 0; l < 4; l++) {
-    uint32_t v[AN_ROWS];
+    for (int l = 0; l < 4; l++)
+      *reinterpret_cast<uint4*>(out[l] + t0) =
+          make_uint4(sub(reduce64(acc[0][l]), bsum[l]), sub(reduce64(acc[1][l]), bsum[l]),
+                     sub(reduce64(acc[2][l]), bsum[l]), sub(reduce64(acc[3][l]), bsum[l]));
+  } else {
 #pragma unroll
-    for (int r = 0; r < AN_ROWS; r++) v[r] = sub(reduce64(acc[r][l]), bsum[l]);
-    if (full && (reinterpret_cast<uintptr_t>(out[l] + row0) & 15) == 0) {
-      *reinterpret_cast<uint4*>(out[l] + row0) = make_uint4(v[0], v[1], v[2], v[3]);
-    } else {
+    for (int r = 0; r < AN_ROWS; r++) {
+      const uint32_t row = t0 + r * stride;
+      if (row < n_rows) {
 #pragma unroll
-      for (int r = 0; r < AN_ROWS; r++)
-        if (row0 + r < n_rows) out[l][row0 + r] = v[r];
+        for (int l = 0; l < 4; l++) out[l][row] = sub(reduce64(acc[r][l]), bsum[l]);
+      }
     }
   }
 }
@@ -255,8 +268,23 @@ void cuda_accumulate_numerators(const uint32_t* const* cols, const uint32_t* idx
                                 uint32_t n_batch, uint32_t n_rows, uint32_t* o0, uint32_t* o1, uint32_t* o2,
                                 uint32_t* o3) {
   if (!n_rows) return;
-  accumulate_numerators_kernel<<<blocks_for((n_rows + AN_ROWS - 1) / AN_ROWS, 256), 256>>>(cols, idx, b, c, n_batch,
-                                                                                         n_rows, o0, o1, o2, o3);
+  // The 128-bit variant needs every column the batch reads, the outputs and the
+  // row count to be multiples of 16 bytes; the column table is device memory, so
+  // its used entries are read back (small, once per call) to decide.
+  bool vec = n_rows % AN_ROWS == 0;
+  for (uint32_t* o : {o0, o1, o2, o3}) vec = vec && (reinterpret_cast<uintptr_t>(o) & 15) == 0;
+  if (vec && n_batch) {
+    std::vector<uint32_t> h_idx(n_batch);
+    if (check_cuda(cudaMemcpy(h_idx.data(), idx, n_batch * 4, cudaMemcpyDeviceToHost), "accumulate: indices") != VS_OK) return;
+    uint32_t n_ptrs = 0;
+    for (uint32_t k : h_idx) n_ptrs = std::max(n_ptrs, k + 1);
+    std::vector<const uint32_t*> h_cols(n_ptrs);
+    if (check_cuda(cudaMemcpy(h_cols.data(), cols, n_ptrs * sizeof(void*), cudaMemcpyDeviceToHost), "accumulate: columns") != VS_OK) return;
+    for (uint32_t k : h_idx) vec = vec && (reinterpret_cast<uintptr_t>(h_cols[k]) & 15) == 0;
+  }
+  const unsigned blocks = blocks_for((n_rows + AN_ROWS - 1) / AN_ROWS, 256);
+  if (vec) accumulate_numerators_kernel<true><<<blocks, 256>>>(cols, idx, b, c, n_batch, n_rows, o0, o1, o2, o3);
+  else accumulate_numerators_kernel<false><<<blocks, 256>>>(cols, idx, b, c, n_batch, n_rows, o0, o1, o2, o3);
   check_cuda(cudaGetLastError(), "cuda_accumulate_numerators");
 }
 void cuda_compute_quotients_combine(const uint32_t* spx, const uint32_t* spy, const uint32_t* fla,
