@@ -296,7 +296,7 @@ __device__ __forceinline__ uint32_t* col_dst(const NttPass& p, uint32_t c) {
 // inverse pass. Every thread commits one copy group per iteration (empty at the
 // end), so "wait until one group is pending" always means "this tile landed".
 template <bool FWD, int M, int C>
-__global__ void __launch_bounds__(1 << (M + C - 5), FWD ? 3 : 2) ntt_pass_kernel(NttPass p, uint32_t n_cols,
+__global__ void __launch_bounds__(1 << (M + C - 5), (FWD && C == 0) ? 3 : 2) ntt_pass_kernel(NttPass p, uint32_t n_cols,
                                                                       uint32_t total) {
   using S = Tile<M, C>;
   extern __shared__ __align__(16) uint32_t pass_sm[];
