@@ -160,6 +160,16 @@ void cuda_compute_quotients_combine(const uint32_t* sample_points_x, const uint3
                                     uint32_t lifting_log_size, uint32_t n_rows, uint32_t* out0, uint32_t* out1,
                                     uint32_t* out2, uint32_t* out3);
 
+/* --- proof-of-work grinding (src/cuda/ffi.rs:632-638, 970-976; cuda/grind.cu, cuda/grind_m31_output.cu) ---
+ * Nonces batch_offset .. batch_offset + n_threads - 1 are tried; the smallest one
+ * whose Blake2s(prefix || nonce_LE) has >= pow_bits trailing zeros in its first 16
+ * bytes is atomicMin'd into *result (device, initialised to UINT64_MAX by the
+ * caller). Asynchronous on the default stream. */
+void cuda_grind_pow(const uint32_t* prefixed_digest, uint64_t* result, uint32_t pow_bits, uint64_t batch_offset,
+                    uint32_t n_threads);
+void cuda_grind_pow_m31_output(const uint32_t* prefixed_digest, uint64_t* result, uint32_t pow_bits,
+                               uint64_t batch_offset, uint32_t n_threads);
+
 /* --- misc (src/cuda/ffi.rs:203-207, 946; cuda/fields.cu, cuda/bit_reverse_wide.cu) --- */
 void cuda_bit_reverse_qm31(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t log_n);
 void cuda_m31_add(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n);
@@ -287,6 +297,24 @@ double vs_engine_now(void* engine);
 
 /* Release cached twiddles and scratch of the current device. */
 int vs_release_caches(void);
+
+/* Fiat–Shamir channel (src/channel.rs:15-185): a Blake2s transcript with the
+ * reference's byte layouts. Digests are 8 LE words; felts are QM31 as 4 words
+ * [a.a, a.b, b.a, b.b]. Host-only state; grind_pow runs the nonce search on the
+ * GPU in batches of 2^26 and returns the smallest passing nonce below max_nonces
+ * (it does not mix the nonce in: call mix_u64, as the reference does). */
+int vs_channel_create(void** channel);
+int vs_channel_destroy(void* channel);
+int vs_channel_state(void* channel, uint8_t* h_state32, uint32_t* n_draws);
+int vs_channel_mix_digest(void* channel, const uint32_t* h_digest8);          /* channel.rs:29-40 */
+int vs_channel_mix_felts(void* channel, const uint32_t* h_felts, uint64_t n_felts); /* channel.rs:44-58 */
+int vs_channel_mix_u64(void* channel, uint64_t value);                          /* channel.rs:120-129 */
+int vs_channel_draw_felt(void* channel, uint32_t* h_out4);                      /* channel.rs:60-86 */
+int vs_channel_draw_number(void* channel, uint64_t bound, uint64_t* out);       /* channel.rs:88-99 */
+int vs_channel_draw_query_indices(void* channel, uint32_t log_domain_size, uint32_t n, uint32_t* h_out); /* :102-116 */
+int vs_channel_pow_prefix(void* channel, uint32_t pow_bits, uint32_t* h_out8);  /* channel.rs:144-152 */
+int vs_channel_verify_pow_nonce(void* channel, uint32_t pow_bits, uint64_t nonce); /* :144-168; 1 valid, 0 not, -1 error */
+int vs_channel_grind_pow(void* channel, uint32_t pow_bits, uint64_t max_nonces, uint64_t* nonce, vs_stream_t stream);
 /* Sets the release threshold of the current device's default stream-ordered
  * memory pool (bytes kept cached across synchronisations; UINT64_MAX never
  * releases). Replaces init_memory_pool (2 GiB) / init_memory_pool_greedy

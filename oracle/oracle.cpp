@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstring>
 #include <functional>
+#include <mutex>
 #include <stdexcept>
 #include <thread>
 
@@ -471,6 +472,49 @@ Hash Channel::state_words() const {
   Hash h;
   for (int i = 0; i < 8; i++) h[i] = le32(&state[4 * i]);
   return h;
+}
+
+Hash Channel::pow_prefix(uint32_t pow_bits) const {  // channel.rs:144-152
+  uint8_t in[52] = {0};
+  const uint32_t magic = 0x12345678u;
+  std::memcpy(in, &magic, 4);
+  std::memcpy(in + 16, state.data(), 32);
+  std::memcpy(in + 48, &pow_bits, 4);
+  const auto d = blake2s_bytes(in, 52);
+  Hash h{};
+  std::memcpy(h.data(), d.data(), 32);
+  return h;
+}
+uint32_t pow_trailing_zeros(const Hash& prefix, uint64_t nonce, bool m31_output) {
+  uint32_t w[10];
+  for (int k = 0; k < 8; k++) w[k] = prefix[k];
+  w[8] = (uint32_t)nonce;
+  w[9] = (uint32_t)(nonce >> 32);
+  Hash r = blake2s_words(w, 10);
+  uint32_t tz = 0;
+  for (int k = 0; k < 4; k++) {
+    uint32_t v = r[k];
+    if (m31_output) v = m31_reduce(v);  // grind_m31_output.cu:47-52 (m31.cuh:9-14)
+    if (v) return tz + (uint32_t)__builtin_ctz(v);
+    tz += 32;
+  }
+  return tz;
+}
+bool Channel::verify_pow_nonce(uint32_t pow_bits, uint64_t nonce) const {  // channel.rs:144-168
+  return pow_trailing_zeros(pow_prefix(pow_bits), nonce, false) >= pow_bits;
+}
+uint64_t pow_grind_min(const Hash& prefix, uint32_t pow_bits, uint64_t offset, uint64_t n, bool m31_output,
+                       int threads) {
+  std::vector<uint64_t> best(std::max(threads, 1), UINT64_MAX);
+  parallel_for(n, threads, [&](uint64_t lo, uint64_t hi) {
+    uint64_t b = UINT64_MAX;
+    for (uint64_t i = lo; i < hi && b == UINT64_MAX; i++)
+      if (pow_trailing_zeros(prefix, offset + i, m31_output) >= pow_bits) b = offset + i;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    best[0] = std::min(best[0], b);
+  });
+  return best[0];
 }
 
 // ------------------------------------------------------------------ FRI

@@ -187,7 +187,16 @@ struct Channel {
   uint64_t draw_number(uint64_t bound);
   std::vector<uint64_t> draw_query_indices(uint32_t log_domain, size_t n);
   Hash state_words() const;
+  // PoW (channel.rs:140-168): prefix = Blake2s(0x12345678_LE || 0^12 || state || pow_bits_LE)
+  Hash pow_prefix(uint32_t pow_bits) const;
+  bool verify_pow_nonce(uint32_t pow_bits, uint64_t nonce) const;
 };
+
+// Trailing zeros of the first 16 bytes (u128 LE) of Blake2s(prefix || nonce_LE)
+// (grind.cu:16-79); m31_output reduces each word mod p first (grind_m31_output.cu).
+uint32_t pow_trailing_zeros(const Hash& prefix, uint64_t nonce, bool m31_output);
+// Smallest nonce in [offset, offset + n) with >= pow_bits trailing zeros, or UINT64_MAX.
+uint64_t pow_grind_min(const Hash& prefix, uint32_t pow_bits, uint64_t offset, uint64_t n, bool m31_output, int threads);
 
 // ---------------------------------------------------------------- FRI
 // Fold twiddles: fri.rs:112-139 + twiddles.cu:23-52 (1/coord(domain.at(bitrev(2i)))).

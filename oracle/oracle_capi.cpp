@@ -193,6 +193,24 @@ void oracle_ch_mix_felts(ChState* s, const uint32_t* f, uint64_t n) {
 void oracle_ch_mix_u64(ChState* s, uint64_t v) { Channel c = load(s); c.mix_u64(v); store(s, c); }
 void oracle_ch_draw_felt(ChState* s, uint32_t* o4) { Channel c = load(s); put(o4, c.draw_felt()); store(s, c); }
 uint64_t oracle_ch_draw_number(ChState* s, uint64_t bound) { Channel c = load(s); uint64_t r = c.draw_number(bound); store(s, c); return r; }
+void oracle_ch_pow_prefix(const ChState* s, uint32_t pow_bits, uint32_t* out8) {
+  Hash h = load(s).pow_prefix(pow_bits);
+  for (int k = 0; k < 8; k++) out8[k] = h[k];
+}
+int oracle_ch_verify_pow(const ChState* s, uint32_t pow_bits, uint64_t nonce) {
+  return load(s).verify_pow_nonce(pow_bits, nonce) ? 1 : 0;
+}
+uint32_t oracle_pow_trailing_zeros(const uint32_t* prefix8, uint64_t nonce, int m31_output) {
+  Hash h{};
+  for (int k = 0; k < 8; k++) h[k] = prefix8[k];
+  return pow_trailing_zeros(h, nonce, m31_output != 0);
+}
+uint64_t oracle_pow_grind_min(const uint32_t* prefix8, uint32_t pow_bits, uint64_t offset, uint64_t n, int m31_output,
+                              int threads) {
+  Hash h{};
+  for (int k = 0; k < 8; k++) h[k] = prefix8[k];
+  return pow_grind_min(h, pow_bits, offset, n, m31_output != 0, threads);
+}
 void oracle_ch_draw_queries(ChState* s, uint32_t log_domain, uint64_t n, uint64_t* out) {
   Channel c = load(s); auto r = c.draw_query_indices(log_domain, n); std::memcpy(out, r.data(), n * 8); store(s, c);
 }

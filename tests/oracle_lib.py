@@ -42,6 +42,8 @@ u8p = C.POINTER(C.c_uint8)
 def _declare(L: C.CDLL) -> None:
     L.oracle_prove.restype = C.c_uint64
     L.oracle_ch_draw_number.restype = C.c_uint64
+    L.oracle_pow_grind_min.restype = C.c_uint64
+    L.oracle_pow_trailing_zeros.restype = C.c_uint32
     L.oracle_m31_mul.restype = C.c_uint32
     L.oracle_m31_inv.restype = C.c_uint32
     L.oracle_bench_commit.restype = C.c_double
@@ -263,10 +265,30 @@ class Channel:
     def state_bytes(self) -> bytes:
         return bytes(self.s.state)
 
+    def pow_prefix(self, pow_bits: int) -> np.ndarray:
+        o = np.empty(8, np.uint32)
+        lib().oracle_ch_pow_prefix(C.byref(self.s), pow_bits, ptr(o))
+        return o
+
+    def verify_pow(self, pow_bits: int, nonce: int) -> bool:
+        return bool(lib().oracle_ch_verify_pow(C.byref(self.s), pow_bits, C.c_uint64(nonce)))
+
     def oods_point(self):
         o = np.empty(8, np.uint32)
         lib().oracle_oods_point(C.byref(self.s), ptr(o))
         return o
+
+
+def pow_trailing_zeros(prefix, nonce: int, m31_output: bool = False) -> int:
+    a = np.ascontiguousarray(prefix, np.uint32)
+    return int(lib().oracle_pow_trailing_zeros(ptr(a), C.c_uint64(nonce), int(m31_output)))
+
+
+def pow_grind_min(prefix, pow_bits: int, offset: int, n: int, m31_output: bool = False, threads: int = 0) -> int:
+    """Smallest nonce in [offset, offset + n) meeting pow_bits, or 2^64 - 1."""
+    a = np.ascontiguousarray(prefix, np.uint32)
+    return int(lib().oracle_pow_grind_min(ptr(a), pow_bits, C.c_uint64(offset), C.c_uint64(n), int(m31_output),
+                                          threads or (os.cpu_count() or 1)))
 
 
 # ----------------------------------------------------------------- FRI / quotient

@@ -107,6 +107,33 @@ uint64_t Channel::draw_number(uint64_t bound) {
   for (int k = 7; k >= 0; k--) raw = (raw << 8) | b[k];
   return raw % bound;
 }
+std::vector<uint32_t> Channel::draw_query_indices(uint32_t log_size, uint32_t n) {
+  const uint32_t mask = log_size >= 32 ? ~0u : (1u << log_size) - 1;
+  std::vector<uint32_t> out;
+  out.reserve(n);
+  while (out.size() < n) {
+    auto b = squeeze();
+    for (int i = 0; i < 8 && out.size() < n; i++) out.push_back(le(&b[4 * i]) & mask);
+  }
+  return out;
+}
+void Channel::mix_u64(uint64_t v) {
+  uint8_t in[40];
+  std::memcpy(in, state.data(), 32);
+  for (int k = 0; k < 8; k++) in[32 + k] = (uint8_t)(v >> (8 * k));
+  state = blake2s(in, 40);
+  n_draws = 0;
+}
+Hash Channel::pow_prefix(uint32_t pow_bits) const {
+  uint8_t in[52] = {0};
+  for (int k = 0; k < 4; k++) in[k] = (uint8_t)(0x12345678u >> (8 * k));
+  std::memcpy(in + 16, state.data(), 32);
+  for (int k = 0; k < 4; k++) in[48 + k] = (uint8_t)(pow_bits >> (8 * k));
+  const auto d = blake2s(in, 52);
+  Hash h{};
+  for (int i = 0; i < 8; i++) h[i] = le(&d[4 * i]);
+  return h;
+}
 
 static Pt rdouble(Pt p, uint32_t k) {
   for (uint32_t i = 0; i < k; i++) p = pmul(p, p);

@@ -80,6 +80,12 @@ struct Channel {
   std::array<uint8_t, 32> squeeze();
   Q draw_felt();
   uint64_t draw_number(uint64_t bound);
+  // channel.rs:102-116: 8 indices per squeeze, word & (2^log_size - 1)
+  std::vector<uint32_t> draw_query_indices(uint32_t log_size, uint32_t n);
+  // channel.rs:120-129: state = Blake2s(state || lo_LE || hi_LE)
+  void mix_u64(uint64_t v);
+  // channel.rs:144-152: Blake2s(0x12345678_LE || 0^12 || state || pow_bits_LE) as words
+  Hash pow_prefix(uint32_t pow_bits) const;
 };
 
 // Circle cosets (circle.rs:101-144).
