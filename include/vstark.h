@@ -298,6 +298,21 @@ double vs_engine_now(void* engine);
 /* Release cached twiddles and scratch of the current device. */
 int vs_release_caches(void);
 
+/* One column group of the reference Cairo prover's trace commitment
+ * (cairo_air/prover.rs:899-1047) with every step on the device: columns in
+ * half-coset natural order (d_cols_hc, n_cols <= 16 at col_stride words) are
+ * permuted to BRT-canonic order (circle.rs:192-204), optionally interpolated to
+ * stwo coefficients (d_coeffs, n_cols x 2^log_n), extended x4 (d_eval_cn, n_cols x
+ * 2^(log_n+2), BRT-canonic), ZK-blinded as column c += h_blind[c] * Z_H for every
+ * nonzero h_blind[c] (prover.rs:924-993; h_blind may be NULL), optionally copied
+ * back to half-coset order (d_eval_hc), and committed with the native leaf of the
+ * group's columns: root (d_root) and 1024-leaf tile roots (d_tile_roots, 2^(log_n+2)
+ * / 1024 hashes, or the root alone below 1024 leaves; may be NULL), as
+ * MerkleTree::commit_root_only_with_subtrees (merkle.rs:360-417). */
+int vs_commit_group_cairo(const uint32_t* d_cols_hc, uint64_t col_stride, uint32_t n_cols, uint32_t log_n,
+                          const uint32_t* h_blind, uint32_t* d_coeffs, uint32_t* d_eval_cn, uint32_t* d_eval_hc,
+                          uint32_t* d_root, uint32_t* d_tile_roots, vs_stream_t stream);
+
 /* Fiat–Shamir channel (src/channel.rs:15-185): a Blake2s transcript with the
  * reference's byte layouts. Digests are 8 LE words; felts are QM31 as 4 words
  * [a.a, a.b, b.a, b.b]. Host-only state; grind_pow runs the nonce search on the

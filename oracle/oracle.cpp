@@ -1027,4 +1027,61 @@ bool deserialize_proof(const uint8_t* data, size_t len, StarkProof& p) {
   return r.ok && r.pos == len;
 }
 
+// ------------------------------------------------------------------ Cairo group commitment
+uint32_t coset_vanishing_at(const Coset& c, CPoint p) {  // circle.rs:238-253
+  const CPoint shp = cp_repeated_double(CP_GENERATOR, 30 - c.log_size);
+  const CPoint r = cp_mul(cp_mul(p, cp_conj(c.initial)), shp);
+  uint32_t x = r.x;
+  for (uint32_t i = 1; i < c.log_size; i++) x = m31_sub(m31_double(m31_mul(x, x)), 1);
+  return x;
+}
+std::vector<uint32_t> zh_eval_domain(uint32_t log_n) {  // cairo_air/prover.rs:924-935
+  const uint32_t log_eval = log_n + 2;
+  const uint64_t N = 1ull << log_eval, half = N / 2;
+  const Coset ho = coset_half_odds(log_eval - 1), hc = coset_half_coset(log_n);
+  std::vector<uint32_t> zh(N);
+  for (uint64_t i = 0; i < N; i++) {
+    const uint64_t b = bit_reverse(i, log_eval);
+    const CPoint p = b < half ? ho.at(b) : cp_conj(ho.at(b - half));
+    zh[i] = coset_vanishing_at(hc, p);
+  }
+  return zh;
+}
+GroupCommit commit_group_cairo(const std::vector<std::vector<uint32_t>>& cols_hc, uint32_t log_n,
+                               const std::vector<uint32_t>& blind, int threads) {
+  GroupCommit g;
+  const uint32_t log_eval = log_n + 2;
+  const StwoTwiddles tw = stwo_twiddles(log_n), te = stwo_twiddles(log_eval);
+  std::vector<uint32_t> zh;
+  for (size_t c = 0; c < cols_hc.size(); c++) {
+    std::vector<uint32_t> cn = permute_hc_natural_to_canonic_brt(cols_hc[c], log_n);
+    std::vector<uint32_t> co = cn;
+    stwo_interpolate(co, tw);
+    g.coeffs.push_back(co);
+    std::vector<uint32_t> ev = stwo_lde(cn, log_n, 2, tw, te);
+    if (c < blind.size() && blind[c]) {
+      if (zh.empty()) zh = zh_eval_domain(log_n);
+      for (size_t i = 0; i < ev.size(); i++) ev[i] = m31_add(ev[i], m31_mul(blind[c], zh[i]));
+    }
+    g.eval_hc.push_back(permute_canonic_brt_to_hc_natural(ev, log_eval));
+    g.eval_cn.push_back(std::move(ev));
+  }
+  std::vector<const uint32_t*> ptrs;
+  for (auto& e : g.eval_cn) ptrs.push_back(e.data());
+  const uint64_t N = 1ull << log_eval;
+  std::vector<Hash> leaves(N);
+  parallel_for(N, threads, [&](uint64_t lo, uint64_t hi) {
+    std::vector<uint32_t> row(ptrs.size());
+    for (uint64_t i = lo; i < hi; i++) {
+      for (size_t c = 0; c < ptrs.size(); c++) row[c] = ptrs[c][i];
+      leaves[i] = leaf_hash_capped(row.data(), (uint32_t)ptrs.size());
+    }
+  });
+  auto layers = merkle_layers(leaves);  // layers[0] = leaves
+  g.root = layers.back()[0];
+  if (N < 1024) g.tile_roots = {g.root};
+  else g.tile_roots = layers[10];
+  return g;
+}
+
 }  // namespace vso

@@ -225,6 +225,20 @@ QM31 eval_at_oods_from_coeffs(const std::vector<uint32_t>& coeffs, OodsPoint z);
 void compute_line_coeffs(OodsPoint z, QM31 v, QM31& a, QM31& b);
 CPoint canonic_domain_point(uint64_t j, uint32_t log_eval);  // cairo_air/prover.rs:161-165
 
+// ---------------------------------------------------------------- Cairo group commitment
+// circle.rs:232-253: vanishing polynomial of a coset at a point
+uint32_t coset_vanishing_at(const Coset& c, CPoint p);
+// cairo_air/prover.rs:924-935: Z_H of half_coset(log_n) at the BRT-canonic points of the 4x domain
+std::vector<uint32_t> zh_eval_domain(uint32_t log_n);
+// cairo_air/prover.rs:955-1047 for one group (<= 16 columns), with merkle.rs:360-417
+struct GroupCommit {
+  std::vector<std::vector<uint32_t>> coeffs, eval_cn, eval_hc;
+  Hash root;
+  std::vector<Hash> tile_roots;
+};
+GroupCommit commit_group_cairo(const std::vector<std::vector<uint32_t>>& cols_hc, uint32_t log_n,
+                               const std::vector<uint32_t>& blind, int threads);
+
 // ---------------------------------------------------------------- Fibonacci AIR + prover
 // air.rs:16-25 (additive recurrence, t0 = a, t1 = b)
 std::vector<uint32_t> fibonacci_trace(uint32_t a, uint32_t b, uint32_t log_n);

@@ -378,3 +378,28 @@ double oracle_bench_fri(const uint32_t* const src[4], uint32_t log_n, const uint
 }
 
 }  // extern "C"
+
+extern "C" void oracle_commit_group_cairo(const uint32_t* cols_hc, uint32_t n_cols, uint32_t log_n, const uint32_t* blind,
+                                          uint32_t* coeffs, uint32_t* eval_cn, uint32_t* eval_hc, uint32_t* root,
+                                          uint32_t* tile_roots, int threads) {
+  const uint64_t n = 1ull << log_n, N = n << 2;
+  std::vector<std::vector<uint32_t>> cols(n_cols);
+  for (uint32_t c = 0; c < n_cols; c++) cols[c].assign(cols_hc + c * n, cols_hc + (c + 1) * n);
+  std::vector<uint32_t> b(blind, blind + n_cols);
+  GroupCommit g = commit_group_cairo(cols, log_n, b, threads);
+  for (uint32_t c = 0; c < n_cols; c++) {
+    std::copy(g.coeffs[c].begin(), g.coeffs[c].end(), coeffs + c * n);
+    std::copy(g.eval_cn[c].begin(), g.eval_cn[c].end(), eval_cn + c * N);
+    std::copy(g.eval_hc[c].begin(), g.eval_hc[c].end(), eval_hc + c * N);
+  }
+  for (int k = 0; k < 8; k++) root[k] = g.root[k];
+  for (size_t t = 0; t < g.tile_roots.size(); t++)
+    for (int k = 0; k < 8; k++) tile_roots[8 * t + k] = g.tile_roots[t][k];
+}
+extern "C" void oracle_zh_eval_domain(uint32_t log_n, uint32_t* out) {
+  auto z = zh_eval_domain(log_n);
+  std::copy(z.begin(), z.end(), out);
+}
+extern "C" uint32_t oracle_coset_vanishing_half_coset(uint32_t log_n, uint32_t x, uint32_t y) {
+  return coset_vanishing_at(coset_half_coset(log_n), CPoint{x, y});
+}

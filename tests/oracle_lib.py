@@ -44,6 +44,7 @@ def _declare(L: C.CDLL) -> None:
     L.oracle_ch_draw_number.restype = C.c_uint64
     L.oracle_pow_grind_min.restype = C.c_uint64
     L.oracle_pow_trailing_zeros.restype = C.c_uint32
+    L.oracle_coset_vanishing_half_coset.restype = C.c_uint32
     L.oracle_m31_mul.restype = C.c_uint32
     L.oracle_m31_inv.restype = C.c_uint32
     L.oracle_bench_commit.restype = C.c_double
@@ -140,6 +141,33 @@ def stwo_lde_columns(cols: np.ndarray, log_n: int, blowup: int = 2, threads: int
     out = np.empty((nc, 1 << (log_n + blowup)), np.uint32)
     lib().oracle_stwo_lde_columns(ptr(cols), nc, log_n, blowup, ptr(out), threads)
     return out
+
+
+def zh_eval_domain(log_n: int) -> np.ndarray:
+    """Z_H of half_coset(log_n) at the BRT-canonic points of the 4x evaluation domain."""
+    out = np.empty(1 << (log_n + 2), np.uint32)
+    lib().oracle_zh_eval_domain(log_n, ptr(out))
+    return out
+
+
+def coset_vanishing_half_coset(log_n: int, x: int, y: int) -> int:
+    return int(lib().oracle_coset_vanishing_half_coset(log_n, x, y))
+
+
+def commit_group_cairo(cols_hc: np.ndarray, log_n: int, blind=None, threads: int = 8) -> dict:
+    """One Cairo column group: coefficients, blinded BRT-canonic LDE, its half-coset
+    copy, the capped-leaf root and the 1024-leaf tile roots."""
+    cols_hc = np.ascontiguousarray(cols_hc, np.uint32)
+    nc, n = cols_hc.shape
+    N = n << 2
+    b = np.zeros(nc, np.uint32) if blind is None else np.ascontiguousarray(blind, np.uint32)
+    coeffs = np.empty((nc, n), np.uint32)
+    ev_cn, ev_hc = np.empty((nc, N), np.uint32), np.empty((nc, N), np.uint32)
+    root = np.empty(8, np.uint32)
+    tiles = np.empty((max(1, N // 1024), 8), np.uint32)
+    lib().oracle_commit_group_cairo(ptr(cols_hc), nc, log_n, ptr(b), ptr(coeffs), ptr(ev_cn), ptr(ev_hc), ptr(root),
+                                    ptr(tiles), threads)
+    return {"coeffs": coeffs, "eval_cn": ev_cn, "eval_hc": ev_hc, "root": root, "tile_roots": tiles}
 
 
 def bit_reverse(d: np.ndarray, log_n: int) -> np.ndarray:

@@ -47,6 +47,7 @@ uint64_t vs_launch_count(void) { return g_launches.load(std::memory_order_relaxe
 
 int vs_release_caches(void) {
   clear_error();
+  release_zh_tables();
   return release_twiddles();
 }
 

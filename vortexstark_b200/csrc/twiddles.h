@@ -39,6 +39,8 @@ int get_twiddles(int kind, uint32_t log_n, const TwiddleSet** out, cudaStream_t 
 // (half_coset -> y, half_odds -> x), cached per (device, which, log_n).
 int get_fold_twiddles(int which, uint32_t log_n, const uint32_t** out, cudaStream_t st);
 int release_twiddles();
+// Frees the cached vanishing-polynomial tables of the Cairo group commit (cairo.cu).
+void release_zh_tables();
 
 int launch_batch_inverse(const uint32_t* in, uint32_t* out, uint64_t n, cudaStream_t st);
 int launch_coset_points(cpt initial, cpt step, uint32_t* ox, uint32_t* oy, uint64_t n, cudaStream_t st);
