@@ -313,6 +313,62 @@ int vs_commit_group_cairo(const uint32_t* d_cols_hc, uint64_t col_stride, uint32
                           const uint32_t* h_blind, uint32_t* d_coeffs, uint32_t* d_eval_cn, uint32_t* d_eval_hc,
                           uint32_t* d_root, uint32_t* d_tile_roots, vs_stream_t stream);
 
+/* Circle polynomials in the stwo coefficient basis evaluated at QM31 points
+ * (oods.rs:133-161, eval_at_oods_from_coeffs, which the reference runs on the
+ * host per column). h_cols: host array of n_cols device pointers, 2^log_len
+ * coefficients each; h_points: n_points (<= 2) points as 8 words (x QM31, y
+ * QM31); h_out: n_cols x n_points QM31 (4 words), column-major over points.
+ * Synchronises the stream. */
+int vs_eval_at_oods_points(const uint32_t* const* h_cols, uint32_t n_cols, uint32_t log_len,
+                           const uint32_t* h_points, uint32_t n_points, uint32_t* h_out, vs_stream_t stream);
+
+/* The reference Cairo prover's tail after the trace and interaction commitments
+ * (cairo_air/prover.rs:1937-2438), device-resident:
+ *   AIR quotient (4 limbs, half-coset natural) -> BRT-canonic -> SoA4 commitment
+ *   with 1024-leaf tile roots, mixed; OODS point z from the channel, z_next one
+ *   trace step on; trace columns at z / z_next from their coefficients (plus
+ *   r * Z_H at the point for blinded columns), interaction columns from the first
+ *   2^log_n stwo coefficients of their evaluations, quotient limbs from all
+ *   coefficients; sampled values mixed in flatten_cols order; OODS alpha drawn;
+ *   DEEP quotient numerators over [trace, quotient, interaction] columns for z
+ *   and [trace, interaction] for z_next with alpha-power line coefficients;
+ *   combination on the BRT-canonic domain; SoA4 commitment with tile roots,
+ *   mixed; FRI circle fold (twiddles 1/y of the canonic points) and committed
+ *   line folds down to 8 values; last-layer line-polynomial coefficients (BRT
+ *   order) mixed.
+ * The channel is advanced exactly as the reference's. Device outputs left NULL
+ * are kept internally; host arrays left NULL are not written. */
+typedef struct {
+  uint32_t log_n;         /* trace rows 2^log_n (2..26); evaluation domain 2^(log_n+2) */
+  uint32_t n_trace;       /* trace columns (1..1024) */
+  uint32_t n_interaction; /* interaction component columns (0..1024) */
+  uint32_t pad;
+  const uint32_t* const* trace_coeffs;      /* host array of device pointers: 2^log_n stwo coefficients */
+  const uint32_t* zk_scalars;               /* host: blinding scalar per trace column (0 = none), or NULL */
+  const uint32_t* const* trace_evals;       /* host array of device pointers: BRT-canonic evaluations */
+  const uint32_t* const* interaction_evals; /* host array of device pointers: BRT-canonic evaluations */
+  const uint32_t* quotient_hc[4];           /* device: AIR quotient limbs, half-coset natural order */
+  uint32_t* quotient_cn[4];                 /* device out (optional): quotient limbs, BRT-canonic */
+  uint32_t* oods_quotient[4];               /* device out (optional): DEEP quotient limbs, BRT-canonic */
+  uint32_t* quotient_tile_roots;            /* device out (optional): max(1, N/1024) hashes */
+  uint32_t* oods_tile_roots;                /* device out (optional): max(1, N/1024) hashes */
+  uint32_t* trace_at_z;                     /* host out (optional): 4 x n_trace */
+  uint32_t* trace_at_z_next;                /* host out (optional): 4 x n_trace */
+  uint32_t* interaction_at_z;               /* host out (optional): 4 x n_interaction */
+  uint32_t* interaction_at_z_next;          /* host out (optional): 4 x n_interaction */
+  uint32_t quotient_root[8];
+  uint32_t oods_point[8];     /* z.x then z.y (QM31 each) */
+  uint32_t quotient_at_z[16]; /* 4 limbs x QM31 */
+  uint32_t oods_alpha[4];
+  uint32_t oods_root[8];
+  uint32_t n_fri_roots;       /* committed line layers: log_n - 2 */
+  uint32_t fri_roots[32 * 8];
+  uint32_t fri_alphas[32 * 4]; /* [0] circle fold, then one per line fold (log_n - 1 in all) */
+  uint32_t last_layer[8 * 4];  /* the 8 final evaluations */
+  uint32_t last_layer_coeffs[8 * 4];
+} vs_cairo_oods_fri_io;
+int vs_cairo_oods_fri(void* channel, vs_cairo_oods_fri_io* io, vs_stream_t stream);
+
 /* Fiat–Shamir channel (src/channel.rs:15-185): a Blake2s transcript with the
  * reference's byte layouts. Digests are 8 LE words; felts are QM31 as 4 words
  * [a.a, a.b, b.a, b.b]. Host-only state; grind_pow runs the nonce search on the

@@ -1084,4 +1084,164 @@ GroupCommit commit_group_cairo(const std::vector<std::vector<uint32_t>>& cols_hc
   return g;
 }
 
+
+// ------------------------------------------------------------------ Cairo OODS + FRI tail
+static QM31 qm_double_x(QM31 x) {  // oods.rs double_x_qm31: 2x^2 - 1
+  QM31 x2 = qm_mul(x, x);
+  return qm_sub(qm_add(x2, x2), qm_m31(1));
+}
+// merkle.rs:294-330: SoA4 leaves, root and 1024-leaf tile roots (root alone below 1024)
+static void soa4_root_tiles(const std::vector<uint32_t>* c, Hash& root, std::vector<Hash>& tiles, int threads) {
+  const uint64_t n = c[0].size();
+  std::vector<Hash> leaves(n);
+  parallel_for(n, threads, [&](uint64_t lo, uint64_t hi) {
+    for (uint64_t i = lo; i < hi; i++) {
+      uint32_t w[4] = {c[0][i], c[1][i], c[2][i], c[3][i]};
+      leaves[i] = blake2s_words(w, 4);
+    }
+  });
+  auto layers = merkle_layers(std::move(leaves));
+  root = layers.back()[0];
+  tiles = n < 1024 ? std::vector<Hash>{root} : layers[10];
+}
+CairoOodsFri cairo_oods_fri(Channel& ch, uint32_t log_n, const std::vector<std::vector<uint32_t>>& trace_coeffs,
+                            const std::vector<uint32_t>& zk, const std::vector<std::vector<uint32_t>>& trace_evals,
+                            const std::vector<std::vector<uint32_t>>& inter_evals,
+                            const std::vector<std::vector<uint32_t>>& quot_hc, int threads) {
+  CairoOodsFri r;
+  const uint32_t log_eval = log_n + 2;
+  const uint64_t n = 1ull << log_n, N = 1ull << log_eval;
+  const size_t nt = trace_coeffs.size(), ni = inter_evals.size();
+  const StwoTwiddles te = stwo_twiddles(log_eval);
+  // AIR quotient: half-coset natural -> BRT-canonic, SoA4 commitment (prover.rs:1937-1971)
+  std::vector<uint32_t> hq[4];
+  for (int k = 0; k < 4; k++) hq[k] = permute_hc_natural_to_canonic_brt(quot_hc[k], log_eval);
+  soa4_root_tiles(hq, r.quotient_root, r.quotient_tiles, threads);
+  ch.mix_digest(r.quotient_root);
+  // OODS point and its successor on the trace domain (prover.rs:1975-1985)
+  const OodsPoint z = oods_point_from_channel(ch);
+  const CPoint step = cp_repeated_double(CP_GENERATOR, 31 - log_n);
+  const OodsPoint zn{qm_sub(qm_scale(z.x, step.x), qm_scale(z.y, step.y)),
+                     qm_add(qm_scale(z.x, step.y), qm_scale(z.y, step.x))};
+  r.z = z;
+  QM31 zh_z = z.x, zh_zn = zn.x;  // oods.rs:285-291
+  for (uint32_t i = 1; i < log_n; i++) { zh_z = qm_double_x(zh_z); zh_zn = qm_double_x(zh_zn); }
+  // trace columns at z and z_next, blinding added as r * Z_H (prover.rs:1987-2001)
+  for (size_t c = 0; c < nt; c++) {
+    QM31 vz = eval_at_oods_from_coeffs(trace_coeffs[c], z), vn = eval_at_oods_from_coeffs(trace_coeffs[c], zn);
+    if (c < zk.size() && zk[c]) {
+      vz = qm_add(vz, qm_scale(zh_z, zk[c]));
+      vn = qm_add(vn, qm_scale(zh_zn, zk[c]));
+    }
+    r.trace_at_z.push_back(vz);
+    r.trace_at_z_next.push_back(vn);
+  }
+  // interaction columns: stwo iNTT of the evaluations, first n coefficients (prover.rs:2037-2048)
+  for (size_t c = 0; c < ni; c++) {
+    std::vector<uint32_t> co = inter_evals[c];
+    stwo_interpolate(co, te);
+    co.resize(n);
+    r.inter_at_z.push_back(eval_at_oods_from_coeffs(co, z));
+    r.inter_at_z_next.push_back(eval_at_oods_from_coeffs(co, zn));
+  }
+  // AIR quotient limbs at z from all N coefficients (prover.rs:2053-2065)
+  for (int k = 0; k < 4; k++) {
+    std::vector<uint32_t> co = hq[k];
+    stwo_interpolate(co, te);
+    r.quotient_at_z[k] = eval_at_oods_from_coeffs(co, z);
+  }
+  {  // sampled values in flatten_cols order (prover.rs:2067-2092)
+    std::vector<QM31> all;
+    for (size_t c = 0; c < nt; c++) { all.push_back(r.trace_at_z[c]); all.push_back(r.trace_at_z_next[c]); }
+    for (size_t c = 0; c < ni; c++) { all.push_back(r.inter_at_z[c]); all.push_back(r.inter_at_z_next[c]); }
+    for (int k = 0; k < 4; k++) all.push_back(r.quotient_at_z[k]);
+    ch.mix_felts(all);
+  }
+  const QM31 alpha = ch.draw_felt();
+  r.oods_alpha = alpha;
+  // line coefficients weighted by powers of alpha (prover.rs:2095-2150)
+  std::vector<QM31> bz, cz, bn, cn;
+  QM31 lin_z{{0, 0, 0, 0}}, lin_n{{0, 0, 0, 0}}, ap = qm_m31(1);
+  auto push = [&](OodsPoint p, QM31 v, std::vector<QM31>& b, std::vector<QM31>& c, QM31& lin) {
+    QM31 a, bb;
+    compute_line_coeffs(p, v, a, bb);
+    b.push_back(qm_mul(ap, a));
+    c.push_back(ap);
+    lin = qm_add(lin, qm_mul(ap, bb));
+    ap = qm_mul(ap, alpha);
+  };
+  for (size_t c = 0; c < nt; c++) push(z, r.trace_at_z[c], bz, cz, lin_z);
+  for (int k = 0; k < 4; k++) push(z, r.quotient_at_z[k], bz, cz, lin_z);
+  for (size_t c = 0; c < ni; c++) push(z, r.inter_at_z[c], bz, cz, lin_z);
+  for (size_t c = 0; c < nt; c++) push(zn, r.trace_at_z_next[c], bn, cn, lin_n);
+  for (size_t c = 0; c < ni; c++) push(zn, r.inter_at_z_next[c], bn, cn, lin_n);
+  // numerators over [trace, quotient, interaction] columns (prover.rs:2152-2207)
+  std::vector<const uint32_t*> cols;
+  for (auto& e : trace_evals) cols.push_back(e.data());
+  for (int k = 0; k < 4; k++) cols.push_back(hq[k].data());
+  for (auto& e : inter_evals) cols.push_back(e.data());
+  std::vector<uint32_t> idx_z, idx_n;
+  for (uint32_t i = 0; i < nt + 4 + ni; i++) idx_z.push_back(i);
+  for (uint32_t i = 0; i < nt; i++) idx_n.push_back(i);
+  for (uint32_t i = 0; i < ni; i++) idx_n.push_back((uint32_t)(nt + 4 + i));
+  std::vector<QM31> num_z(N), num_n(N);
+  parallel_for(N, threads, [&](uint64_t lo, uint64_t hi) {
+    std::vector<const uint32_t*> sub(cols.size());
+    for (size_t c = 0; c < cols.size(); c++) sub[c] = cols[c] + lo;
+    accumulate_numerators(sub, idx_z, bz, cz, hi - lo, num_z.data() + lo);
+    accumulate_numerators(sub, idx_n, bn, cn, hi - lo, num_n.data() + lo);
+  });
+  // BRT-canonic domain points and the combination (prover.rs:2213-2266)
+  std::vector<uint32_t> dx(N), dy(N);
+  for (uint64_t i = 0; i < N; i++) {
+    const CPoint p = canonic_domain_point(bit_reverse(i, log_eval), log_eval);
+    dx[i] = p.x;
+    dy[i] = p.y;
+  }
+  std::vector<QuotAcc> accs{{z.x, z.y, lin_z, num_z.data(), log_eval}, {zn.x, zn.y, lin_n, num_n.data(), log_eval}};
+  std::vector<QM31> oq(N);
+  quotients_combine(accs, dx.data(), dy.data(), log_eval, N, oq.data());
+  for (int k = 0; k < 4; k++) {
+    r.oods_q[k].resize(N);
+    for (uint64_t i = 0; i < N; i++) r.oods_q[k][i] = oq[i].v[k];
+  }
+  soa4_root_tiles(r.oods_q, r.oods_root, r.oods_tiles, threads);
+  ch.mix_digest(r.oods_root);
+  // FRI: circle fold with twiddles 1/y of the canonic points (prover.rs:2321-2340)
+  const QM31 fa = ch.draw_felt();
+  r.fri_alphas.push_back(fa);
+  const Coset ho = coset_half_odds(log_eval - 1);
+  const std::vector<uint32_t> ctw = fold_twiddles(Coset{ho.initial, ho.step, log_eval}, true);
+  std::vector<QM31> line(N / 2, QM31{{0, 0, 0, 0}});
+  fold_circle_into_line(line.data(), oq.data(), ctw.data(), fa, N / 2);
+  // committed line folds down to 2^3 values (prover.rs:2353-2381)
+  uint32_t cur = log_eval - 1;
+  while (cur > 3) {
+    std::vector<uint32_t> soa[4];
+    for (int k = 0; k < 4; k++) {
+      soa[k].resize(line.size());
+      for (size_t i = 0; i < line.size(); i++) soa[k][i] = line[i].v[k];
+    }
+    const uint32_t* cp[4] = {soa[0].data(), soa[1].data(), soa[2].data(), soa[3].data()};
+    const Hash root = merkle_root_soa4(cp, line.size(), threads);
+    ch.mix_digest(root);
+    r.fri_roots.push_back(root);
+    const QM31 a = ch.draw_felt();
+    r.fri_alphas.push_back(a);
+    const std::vector<uint32_t> tw = fold_twiddles(coset_half_odds(cur), false);
+    std::vector<QM31> nx(line.size() / 2);
+    fold_line(nx.data(), line.data(), tw.data(), a, nx.size());
+    line.swap(nx);
+    cur--;
+  }
+  r.last_layer = line;
+  const std::vector<QM31> nat = last_layer_poly_coeffs(line);
+  r.last_layer_coeffs.assign(nat.size(), QM31{{0, 0, 0, 0}});
+  uint32_t lb = 0;
+  while ((1ull << lb) < nat.size()) lb++;
+  for (size_t i = 0; i < nat.size(); i++) r.last_layer_coeffs[bit_reverse(i, lb)] = nat[i];
+  ch.mix_felts(r.last_layer_coeffs);
+  return r;
+}
+
 }  // namespace vso

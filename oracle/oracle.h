@@ -239,6 +239,30 @@ struct GroupCommit {
 GroupCommit commit_group_cairo(const std::vector<std::vector<uint32_t>>& cols_hc, uint32_t log_n,
                                const std::vector<uint32_t>& blind, int threads);
 
+// ---------------------------------------------------------------- Cairo OODS + FRI tail
+// cairo_air/prover.rs:1937-2438: AIR quotient commitment, OODS sampling of the
+// trace / interaction / quotient columns, DEEP (OODS) quotient, its commitment
+// and the FRI fold chain down to 8 values, ending with the mix of the last-layer
+// line-polynomial coefficients.
+struct CairoOodsFri {
+  Hash quotient_root;
+  std::vector<Hash> quotient_tiles;
+  OodsPoint z;
+  std::vector<QM31> trace_at_z, trace_at_z_next, inter_at_z, inter_at_z_next;
+  QM31 quotient_at_z[4];
+  QM31 oods_alpha;
+  std::vector<uint32_t> oods_q[4];  // BRT-canonic SoA
+  Hash oods_root;
+  std::vector<Hash> oods_tiles;
+  std::vector<QM31> fri_alphas;     // [0] = circle fold
+  std::vector<Hash> fri_roots;      // committed line layers, log_eval - 1 down to 4
+  std::vector<QM31> last_layer, last_layer_coeffs;  // 8 evaluations; 8 coefficients in BRT order
+};
+CairoOodsFri cairo_oods_fri(Channel& ch, uint32_t log_n, const std::vector<std::vector<uint32_t>>& trace_coeffs,
+                            const std::vector<uint32_t>& zk, const std::vector<std::vector<uint32_t>>& trace_evals,
+                            const std::vector<std::vector<uint32_t>>& inter_evals,
+                            const std::vector<std::vector<uint32_t>>& quot_hc, int threads);
+
 // ---------------------------------------------------------------- Fibonacci AIR + prover
 // air.rs:16-25 (additive recurrence, t0 = a, t1 = b)
 std::vector<uint32_t> fibonacci_trace(uint32_t a, uint32_t b, uint32_t log_n);

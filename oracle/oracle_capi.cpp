@@ -403,3 +403,42 @@ extern "C" void oracle_zh_eval_domain(uint32_t log_n, uint32_t* out) {
 extern "C" uint32_t oracle_coset_vanishing_half_coset(uint32_t log_n, uint32_t x, uint32_t y) {
   return coset_vanishing_at(coset_half_coset(log_n), CPoint{x, y});
 }
+
+// Cairo OODS + FRI tail. Flat inputs: trace_coeffs nt x 2^log_n, trace_evals nt x N,
+// inter_evals ni x N, quot_hc 4 x N (N = 2^(log_n+2)). Outputs as in CairoOodsFri;
+// tiles hold max(1, N/1024) hashes, fri_roots log_n - 2, fri_alphas log_n - 1.
+extern "C" void oracle_cairo_oods_fri(ChState* s, uint32_t log_n, const uint32_t* trace_coeffs, uint32_t nt,
+                                      const uint32_t* zk, const uint32_t* trace_evals, const uint32_t* inter_evals,
+                                      uint32_t ni, const uint32_t* quot_hc, uint32_t* quotient_root,
+                                      uint32_t* quotient_tiles, uint32_t* z8, uint32_t* trace_at_z,
+                                      uint32_t* trace_at_zn, uint32_t* inter_at_z, uint32_t* inter_at_zn,
+                                      uint32_t* quot_at_z16, uint32_t* alpha4, uint32_t* oods_q, uint32_t* oods_root,
+                                      uint32_t* oods_tiles, uint32_t* fri_roots, uint32_t* fri_alphas,
+                                      uint32_t* last32, uint32_t* coeffs32, int threads) {
+  const uint64_t n = 1ull << log_n, N = n << 2;
+  std::vector<std::vector<uint32_t>> tc(nt), te(nt), ie(ni), qh(4);
+  for (uint32_t c = 0; c < nt; c++) {
+    tc[c].assign(trace_coeffs + c * n, trace_coeffs + (c + 1) * n);
+    te[c].assign(trace_evals + c * N, trace_evals + (c + 1) * N);
+  }
+  for (uint32_t c = 0; c < ni; c++) ie[c].assign(inter_evals + c * N, inter_evals + (c + 1) * N);
+  for (int k = 0; k < 4; k++) qh[k].assign(quot_hc + k * N, quot_hc + (k + 1) * N);
+  std::vector<uint32_t> z(zk, zk + nt);
+  Channel ch = load(s);
+  CairoOodsFri r = cairo_oods_fri(ch, log_n, tc, z, te, ie, qh, threads);
+  store(s, ch);
+  put_hash(quotient_root, r.quotient_root);
+  for (size_t t = 0; t < r.quotient_tiles.size(); t++) put_hash(quotient_tiles + 8 * t, r.quotient_tiles[t]);
+  put(z8, r.z.x);
+  put(z8 + 4, r.z.y);
+  for (uint32_t c = 0; c < nt; c++) { put(trace_at_z + 4 * c, r.trace_at_z[c]); put(trace_at_zn + 4 * c, r.trace_at_z_next[c]); }
+  for (uint32_t c = 0; c < ni; c++) { put(inter_at_z + 4 * c, r.inter_at_z[c]); put(inter_at_zn + 4 * c, r.inter_at_z_next[c]); }
+  for (int k = 0; k < 4; k++) put(quot_at_z16 + 4 * k, r.quotient_at_z[k]);
+  put(alpha4, r.oods_alpha);
+  for (int k = 0; k < 4; k++) std::copy(r.oods_q[k].begin(), r.oods_q[k].end(), oods_q + k * N);
+  put_hash(oods_root, r.oods_root);
+  for (size_t t = 0; t < r.oods_tiles.size(); t++) put_hash(oods_tiles + 8 * t, r.oods_tiles[t]);
+  for (size_t i = 0; i < r.fri_roots.size(); i++) put_hash(fri_roots + 8 * i, r.fri_roots[i]);
+  for (size_t i = 0; i < r.fri_alphas.size(); i++) put(fri_alphas + 4 * i, r.fri_alphas[i]);
+  for (int i = 0; i < 8; i++) { put(last32 + 4 * i, r.last_layer[i]); put(coeffs32 + 4 * i, r.last_layer_coeffs[i]); }
+}

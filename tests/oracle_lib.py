@@ -307,6 +307,41 @@ class Channel:
         return o
 
 
+def cairo_oods_fri(ch: "Channel", log_n: int, trace_coeffs, zk, trace_evals, inter_evals, quot_hc,
+                   threads: int = 8) -> dict:
+    """Cairo prover tail (quotient commitment, OODS, DEEP quotient, FRI); advances ch."""
+    n, N = 1 << log_n, 4 << log_n
+    tc = np.ascontiguousarray(trace_coeffs, np.uint32).reshape(-1, n)
+    nt = tc.shape[0]
+    te = np.ascontiguousarray(trace_evals, np.uint32).reshape(nt, N)
+    ie = np.ascontiguousarray(inter_evals, np.uint32).reshape(-1, N)
+    ni = ie.shape[0]
+    qh = np.ascontiguousarray(quot_hc, np.uint32).reshape(4, N)
+    z = np.zeros(nt, np.uint32) if zk is None else np.ascontiguousarray(zk, np.uint32)
+    nt_ = max(1, N // 1024)
+    out = {
+        "quotient_root": np.empty(8, np.uint32), "quotient_tiles": np.empty((nt_, 8), np.uint32),
+        "oods_point": np.empty(8, np.uint32), "trace_at_z": np.empty((nt, 4), np.uint32),
+        "trace_at_z_next": np.empty((nt, 4), np.uint32), "interaction_at_z": np.empty((max(ni, 1), 4), np.uint32),
+        "interaction_at_z_next": np.empty((max(ni, 1), 4), np.uint32), "quotient_at_z": np.empty((4, 4), np.uint32),
+        "oods_alpha": np.empty(4, np.uint32), "oods_quotient": np.empty((4, N), np.uint32),
+        "oods_root": np.empty(8, np.uint32), "oods_tiles": np.empty((nt_, 8), np.uint32),
+        "fri_roots": np.empty((max(log_n - 2, 1), 8), np.uint32), "fri_alphas": np.empty((log_n - 1, 4), np.uint32),
+        "last_layer": np.empty((8, 4), np.uint32), "last_layer_coeffs": np.empty((8, 4), np.uint32),
+    }
+    o = out
+    lib().oracle_cairo_oods_fri(C.byref(ch.s), log_n, ptr(tc), nt, ptr(z), ptr(te), ptr(ie if ni else np.zeros(1, np.uint32)),
+                                ni, ptr(qh), ptr(o["quotient_root"]), ptr(o["quotient_tiles"]), ptr(o["oods_point"]),
+                                ptr(o["trace_at_z"]), ptr(o["trace_at_z_next"]), ptr(o["interaction_at_z"]),
+                                ptr(o["interaction_at_z_next"]), ptr(o["quotient_at_z"]), ptr(o["oods_alpha"]),
+                                ptr(o["oods_quotient"]), ptr(o["oods_root"]), ptr(o["oods_tiles"]), ptr(o["fri_roots"]),
+                                ptr(o["fri_alphas"]), ptr(o["last_layer"]), ptr(o["last_layer_coeffs"]), threads)
+    out["interaction_at_z"] = out["interaction_at_z"][:ni]
+    out["interaction_at_z_next"] = out["interaction_at_z_next"][:ni]
+    out["fri_roots"] = out["fri_roots"][: log_n - 2]
+    return out
+
+
 def pow_trailing_zeros(prefix, nonce: int, m31_output: bool = False) -> int:
     a = np.ascontiguousarray(prefix, np.uint32)
     return int(lib().oracle_pow_trailing_zeros(ptr(a), C.c_uint64(nonce), int(m31_output)))

@@ -2,6 +2,8 @@
 (vs_commit_group_cairo; cairo_air/prover.rs:899-1047 with merkle.rs:360-417)
 against the CPU oracle, bit-exact: coefficients, blinded BRT-canonic LDE, the
 half-coset copy, root and 1024-leaf tile roots."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -87,3 +89,114 @@ def test_group_commit_rejects_bad_arguments(L):
     assert L.vs_commit_group_cairo(ptr(d), 16, 17, 4, None, None, ptr(out), None, ptr(root), None, None) != 0
     assert L.vs_commit_group_cairo(ptr(d), 8, 1, 4, None, None, ptr(out), None, ptr(root), None, None) != 0
     assert L.vs_commit_group_cairo(ptr(d), 16, 1, 4, u32_host([P]), None, ptr(out), None, ptr(root), None, None) != 0
+
+
+# ------------------------------------------------------------------ evaluation at OODS points
+@pytest.mark.parametrize("log_len,n_cols,n_points", [(2, 1, 1), (5, 3, 2), (11, 2, 2), (12, 5, 1), (16, 3, 2)])
+def test_eval_at_oods_points_matches_oracle(L, log_len, n_cols, n_points):
+    n = 1 << log_len
+    cols = [O.seeded_m31(0x7500 + 7 * log_len + c, n) for c in range(n_cols)]
+    ch = O.Channel()
+    ch.mix_u64(log_len)
+    pts = [ch.oods_point() for _ in range(n_points)]
+    d = [dev(c) for c in cols]
+    hc = (C.c_uint64 * n_cols)(*[ptr(t) for t in d])
+    hp = u32_host(np.concatenate(pts))
+    out = (C.c_uint32 * (4 * n_cols * n_points))()
+    assert L.vs_eval_at_oods_points(hc, n_cols, log_len, hp, n_points, out, None) == 0, L.vs_last_error()
+    got = np.array(out, np.uint32).reshape(n_cols, n_points, 4)
+    for c in range(n_cols):
+        for p in range(n_points):
+            assert np.array_equal(got[c, p], O.eval_at_oods(cols[c], pts[p])), (c, p)
+
+
+# ------------------------------------------------------------------ OODS + FRI tail
+def tail_inputs(log_n, nt, ni, seed):
+    from test_oracle_cairo import cairo_tail_inputs
+    return cairo_tail_inputs(log_n, nt, ni, seed)
+
+
+def run_gpu_tail(inp, log_n):
+    from vortexstark_b200 import api
+    ch = api.Channel()
+    ch.mix_digest(inp["root"])
+    nt = inp["coeffs"].shape[0]
+    tc = [dev(inp["coeffs"][c]) for c in range(nt)]
+    te = [dev(inp["evals"][c]) for c in range(nt)]
+    ie = [dev(inp["inter"][c]) for c in range(inp["inter"].shape[0])]
+    qh = [dev(inp["q_hc"][k]) for k in range(4)]
+    N = 4 << log_n
+    oq = [empty(N) for _ in range(4)]
+    qcn = [empty(N) for _ in range(4)]
+    tiles_q, tiles_o = empty(max(1, N // 1024) * 8), empty(max(1, N // 1024) * 8)
+    KEEP = tc + te + ie + qh + oq + qcn  # noqa: F841 (alive until the call returns)
+    r = api.cairo_oods_fri(ch, log_n, tc, te, ie, qh, zk_scalars=inp["zk"], quotient_cn=qcn, oods_quotient=oq,
+                           quotient_tile_roots=tiles_q, oods_tile_roots=tiles_o)
+    r["oods_quotient"] = np.stack([host(t) for t in oq])
+    r["quotient_cn"] = np.stack([host(t) for t in qcn])
+    r["quotient_tiles"] = host(tiles_q).reshape(-1, 8)
+    r["oods_tiles"] = host(tiles_o).reshape(-1, 8)
+    return r, ch
+
+
+@pytest.mark.parametrize("log_n,nt,ni", [(2, 1, 0), (4, 3, 4), (6, 34, 12), (8, 16, 5), (9, 2, 12)])
+def test_cairo_tail_matches_oracle(L, log_n, nt, ni):
+    inp = tail_inputs(log_n, nt, ni, 0x7600 + log_n)
+    ref_ch = O.Channel()
+    ref_ch.mix_digest(inp["root"])
+    ref = O.cairo_oods_fri(ref_ch, log_n, inp["coeffs"], inp["zk"], inp["evals"], inp["inter"], inp["q_hc"])
+    got, ch = run_gpu_tail(inp, log_n)
+    for k in ("quotient_root", "oods_point", "trace_at_z", "trace_at_z_next", "quotient_at_z", "oods_alpha",
+              "oods_root", "last_layer", "last_layer_coeffs", "oods_quotient", "quotient_tiles", "oods_tiles"):
+        assert np.array_equal(np.array(got[k], np.uint32).reshape(ref[k].shape), ref[k]), k
+    if ni:
+        assert np.array_equal(np.array(got["interaction_at_z"], np.uint32), ref["interaction_at_z"])
+        assert np.array_equal(np.array(got["interaction_at_z_next"], np.uint32), ref["interaction_at_z_next"])
+    assert np.array_equal(np.array(got["fri_roots"], np.uint32).reshape(-1, 8), ref["fri_roots"])
+    assert np.array_equal(np.array(got["fri_alphas"], np.uint32), ref["fri_alphas"])
+    assert np.array_equal(got["quotient_cn"], inp["q_cn"])
+    assert ch.state()[0] == ref_ch.state_bytes()
+
+
+def _hc_index_map_dev(log_n: int, device) -> torch.Tensor:
+    n = 1 << log_n
+    k = torch.arange(n, dtype=torch.int64, device=device)
+    cn = torch.where(k % 2 == 0, k // 2, n - 1 - k // 2)
+    rev = torch.zeros_like(cn)
+    for b in range(log_n):
+        rev |= ((cn >> b) & 1) << (log_n - 1 - b)
+    return rev
+
+
+@pytest.mark.parametrize("log_n", [16, 20])
+def test_cairo_tail_full_width_is_low_degree(L, log_n):
+    """34 trace columns committed 16 / 15 / 3 with blinding, 12 interaction columns,
+    an AIR quotient of degree < 2n: at sizes the oracle cannot follow, the DEEP
+    quotient's last FRI layer must still have line degree < 4, and the quotient's
+    BRT-canonic copy must be the inverse permutation of its input."""
+    from vortexstark_b200 import api
+    n, N = 1 << log_n, 4 << log_n
+    devc = torch.device("cuda")
+    cols = api.fill_uniform_m31(torch.empty((34, n), dtype=torch.int32, device=devc), seed=0x7700 + log_n)
+    blind = [(0x2468ACE + 7919 * c) % P for c in range(34)]
+    coeffs = torch.empty((34, n), dtype=torch.int32, device=devc)
+    evals, ch = [], api.Channel()
+    for lo, hi in ((0, 16), (16, 31), (31, 34)):
+        ev, root = api.commit_group_cairo(cols[lo:hi].contiguous(), log_n, blind[lo:hi], coeffs=coeffs[lo:hi])
+        evals.append(ev)
+        ch.mix_digest(host(root))
+    evals = torch.cat(evals)
+    inter_src = api.fill_uniform_m31(torch.empty((12, n), dtype=torch.int32, device=devc), seed=0x7800 + log_n)
+    inter = api.lde_stwo(inter_src, log_n, 2)
+    q_src = api.fill_uniform_m31(torch.empty((4, 2 * n), dtype=torch.int32, device=devc), seed=0x7900 + log_n)
+    q_cn = api.lde_stwo(q_src, log_n + 1, 1)
+    q_hc = q_cn[:, _hc_index_map_dev(log_n + 2, devc)].contiguous()
+    out_cn = [empty(N) for _ in range(4)]
+    torch.cuda.synchronize()
+    r = api.cairo_oods_fri(ch, log_n, list(coeffs), list(evals), list(inter), list(q_hc), zk_scalars=blind,
+                           quotient_cn=out_cn)
+    nat = np.array(r["last_layer_coeffs"], np.uint32)[[0, 4, 2, 6, 1, 5, 3, 7]]
+    assert not nat[4:].any() and nat[:4].any()
+    for k in range(4):
+        assert torch.equal(out_cn[k], q_cn[k])
+    assert len(r["fri_roots"]) == log_n - 2

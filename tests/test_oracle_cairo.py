@@ -96,3 +96,96 @@ def test_group_commit_blinding_adds_r_times_zh():
     c_zh = O.stwo_interpolate(O.zh_eval_domain(log_n), log_n + 2).astype(np.uint64)
     want = (np.concatenate([g0["coeffs"][1], np.zeros(3 * n, np.uint32)]).astype(np.uint64) + 12345 * c_zh) % P
     assert np.array_equal(c_bl, want.astype(np.uint32))
+
+
+# ---------------------------------------------------------------- OODS + FRI tail (prover.rs:1937-2438)
+def hc_index_map(log_n: int) -> np.ndarray:
+    """pos[k] = BRT-canonic position of half-coset natural index k."""
+    n = 1 << log_n
+    k = np.arange(n, dtype=np.uint64)
+    cn = np.where(k % 2 == 0, k // 2, n - 1 - k // 2)
+    rev = np.zeros(n, np.uint64)
+    for b in range(log_n):
+        rev |= ((cn >> np.uint64(b)) & np.uint64(1)) << np.uint64(log_n - 1 - b)
+    return rev.astype(np.int64)
+
+
+def cairo_tail_inputs(log_n: int, nt: int, ni: int, seed: int):
+    """Consistent low-degree inputs: blinded trace group (coefficients + LDE),
+    interaction LDEs of degree < n, AIR quotient limbs of degree < 2n given in
+    half-coset natural order."""
+    n = 1 << log_n
+    rng = np.random.default_rng(seed)
+    cols = rng.integers(0, P, size=(nt, n), dtype=np.uint64).astype(np.uint32)
+    zk = rng.integers(1, P, size=nt, dtype=np.uint64).astype(np.uint32)
+    zk[::3] = 0
+    g = O.commit_group_cairo(cols, log_n, zk)
+    inter = O.stwo_lde_columns(rng.integers(0, P, size=(ni, n), dtype=np.uint64).astype(np.uint32), log_n, 2)
+    q_cn = O.stwo_lde_columns(rng.integers(0, P, size=(4, 2 * n), dtype=np.uint64).astype(np.uint32), log_n + 1, 1)
+    q_hc = q_cn[:, hc_index_map(log_n + 2)]
+    return {"coeffs": g["coeffs"], "zk": zk, "evals": g["eval_cn"], "root": g["root"], "inter": inter,
+            "q_hc": q_hc, "q_cn": q_cn}
+
+
+def brt_to_natural(c: np.ndarray) -> np.ndarray:
+    return c[[int(format(i, "03b")[::-1], 2) for i in range(8)]]
+
+
+def run_tail(inp, log_n):
+    ch = O.Channel()
+    ch.mix_digest(inp["root"])
+    r = O.cairo_oods_fri(ch, log_n, inp["coeffs"], inp["zk"], inp["evals"], inp["inter"], inp["q_hc"])
+    return r, ch
+
+
+@pytest.mark.parametrize("log_n,nt,ni", [(4, 3, 4), (6, 5, 12), (8, 16, 0)])
+def test_cairo_tail_deep_quotient_is_low_degree(log_n, nt, ni):
+    """With consistent inputs the DEEP quotient is a polynomial of degree < 2n, and
+    after the folds the 8-value last layer has line degree < 4 (the reference's own
+    OODS-degree and last-layer round-trip checks, prover.rs:2287-2307, 2391-2423)."""
+    inp = cairo_tail_inputs(log_n, nt, ni, 0x6A00 + log_n)
+    r, _ = run_tail(inp, log_n)
+    N = 4 << log_n
+    for k in range(4):
+        c = O.stwo_interpolate(r["oods_quotient"][k], log_n + 2)
+        assert not c[N // 2:].any()
+    nat = brt_to_natural(r["last_layer_coeffs"])
+    assert not nat[4:].any() and nat[:4].any()
+    assert np.array_equal(r["quotient_root"], O.merkle_root_hashes(r["quotient_tiles"])) or N < 1024
+
+
+def test_cairo_tail_sampled_values_match_the_committed_polynomials():
+    """The trace values at z (coefficients + r * Z_H(z)) equal the blinded LDE's own
+    interpolant at z; the quotient limbs at z equal their interpolant at z."""
+    log_n = 5
+    inp = cairo_tail_inputs(log_n, 4, 4, 0x6B00)
+    r, _ = run_tail(inp, log_n)
+    z = r["oods_point"]
+    for c in range(4):
+        full = O.stwo_interpolate(inp["evals"][c], log_n + 2)
+        assert np.array_equal(O.eval_at_oods(full, z), r["trace_at_z"][c])
+    for k in range(4):
+        full = O.stwo_interpolate(inp["q_cn"][k], log_n + 2)
+        assert np.array_equal(O.eval_at_oods(full, z), r["quotient_at_z"][k])
+    assert r["fri_roots"].shape == (log_n - 2, 8) and r["fri_alphas"].shape == (log_n - 1, 4)
+
+
+def test_cairo_tail_detects_an_inconsistent_column():
+    """A planted error (one trace evaluation changed after its coefficients were
+    taken) gives the DEEP quotient a pole: the last layer is no longer low degree."""
+    log_n = 5
+    inp = cairo_tail_inputs(log_n, 3, 4, 0x6C00)
+    inp["evals"] = inp["evals"].copy()
+    inp["evals"][1, 17] = (int(inp["evals"][1, 17]) + 1) % P
+    r, _ = run_tail(inp, log_n)
+    assert brt_to_natural(r["last_layer_coeffs"])[4:].any()
+
+
+def test_cairo_tail_advances_channel_deterministically():
+    log_n = 4
+    inp = cairo_tail_inputs(log_n, 2, 4, 0x6D00)
+    r1, c1 = run_tail(inp, log_n)
+    r2, c2 = run_tail(inp, log_n)
+    assert c1.state_bytes() == c2.state_bytes()
+    assert np.array_equal(r1["oods_root"], r2["oods_root"])
+    assert c1.state_bytes() != O.Channel().state_bytes()

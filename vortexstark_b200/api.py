@@ -184,3 +184,134 @@ class Engine:
 
     def __exit__(self, *a):
         self.close()
+
+
+# ------------------------------------------------------------------ channel (src/channel.rs)
+class Channel:
+    """Fiat-Shamir transcript held by the library (vs_channel_*)."""
+
+    def __init__(self):
+        self.h = C.c_void_p()
+        check(lib().vs_channel_create(C.byref(self.h)), "vs_channel_create")
+
+    def mix_digest(self, words8) -> None:
+        a = (C.c_uint32 * 8)(*[int(w) for w in words8])
+        check(lib().vs_channel_mix_digest(self.h, a), "vs_channel_mix_digest")
+
+    def mix_felts(self, felts) -> None:
+        flat = [int(w) for f in felts for w in f]
+        a = (C.c_uint32 * max(1, len(flat)))(*flat)
+        check(lib().vs_channel_mix_felts(self.h, a, len(flat) // 4), "vs_channel_mix_felts")
+
+    def mix_u64(self, v: int) -> None:
+        check(lib().vs_channel_mix_u64(self.h, v), "vs_channel_mix_u64")
+
+    def draw_felt(self) -> list[int]:
+        o = (C.c_uint32 * 4)()
+        check(lib().vs_channel_draw_felt(self.h, o), "vs_channel_draw_felt")
+        return list(o)
+
+    def draw_query_indices(self, log_domain: int, n: int) -> list[int]:
+        o = (C.c_uint32 * max(1, n))()
+        check(lib().vs_channel_draw_query_indices(self.h, log_domain, n, o), "vs_channel_draw_query_indices")
+        return list(o)[:n]
+
+    def grind_pow(self, pow_bits: int, max_nonces: int = 1 << 40, stream=None) -> int:
+        nonce = C.c_uint64()
+        check(lib().vs_channel_grind_pow(self.h, pow_bits, max_nonces, C.byref(nonce), _stream(stream)),
+              "vs_channel_grind_pow")
+        return nonce.value
+
+    def state(self) -> tuple[bytes, int]:
+        s = (C.c_uint8 * 32)()
+        n = C.c_uint32()
+        check(lib().vs_channel_state(self.h, s, C.byref(n)), "vs_channel_state")
+        return bytes(s), n.value
+
+    def close(self) -> None:
+        if self.h:
+            lib().vs_channel_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ Cairo trace commitment and tail
+def commit_group_cairo(cols_hc: torch.Tensor, log_n: int, blind=None, coeffs: torch.Tensor | None = None,
+                       eval_hc: torch.Tensor | None = None, tile_roots: torch.Tensor | None = None, stream=None):
+    """One Cairo column group (<= 16 columns, half-coset natural order) -> BRT-canonic
+    x4 LDE, blinded (cairo_air/prover.rs:899-1047). Returns (eval_cn, root)."""
+    n_cols, stride = cols_hc.shape
+    N = 4 << log_n
+    eval_cn = torch.empty((n_cols, N), dtype=torch.int32, device=cols_hc.device)
+    root = torch.empty(8, dtype=torch.int32, device=cols_hc.device)
+    hb = (C.c_uint32 * n_cols)(*[int(b) for b in blind]) if blind is not None else None
+    check(lib().vs_commit_group_cairo(_ptr(cols_hc), stride, n_cols, log_n, hb,
+                                      _ptr(coeffs) if coeffs is not None else None, _ptr(eval_cn),
+                                      _ptr(eval_hc) if eval_hc is not None else None, _ptr(root),
+                                      _ptr(tile_roots) if tile_roots is not None else None, _stream(stream)),
+          "vs_commit_group_cairo")
+    return eval_cn, root
+
+
+class CairoOodsFriIO(C.Structure):
+    """Mirror of vs_cairo_oods_fri_io (include/vstark.h)."""
+    _fields_ = [
+        ("log_n", C.c_uint32), ("n_trace", C.c_uint32), ("n_interaction", C.c_uint32), ("pad", C.c_uint32),
+        ("trace_coeffs", C.c_void_p), ("zk_scalars", C.c_void_p), ("trace_evals", C.c_void_p),
+        ("interaction_evals", C.c_void_p), ("quotient_hc", C.c_void_p * 4), ("quotient_cn", C.c_void_p * 4),
+        ("oods_quotient", C.c_void_p * 4), ("quotient_tile_roots", C.c_void_p), ("oods_tile_roots", C.c_void_p),
+        ("trace_at_z", C.c_void_p), ("trace_at_z_next", C.c_void_p), ("interaction_at_z", C.c_void_p),
+        ("interaction_at_z_next", C.c_void_p), ("quotient_root", C.c_uint32 * 8), ("oods_point", C.c_uint32 * 8),
+        ("quotient_at_z", C.c_uint32 * 16), ("oods_alpha", C.c_uint32 * 4), ("oods_root", C.c_uint32 * 8),
+        ("n_fri_roots", C.c_uint32), ("fri_roots", C.c_uint32 * 256), ("fri_alphas", C.c_uint32 * 128),
+        ("last_layer", C.c_uint32 * 32), ("last_layer_coeffs", C.c_uint32 * 32),
+    ]
+
+
+def cairo_oods_fri(channel: Channel, log_n: int, trace_coeffs, trace_evals, interaction_evals, quotient_hc,
+                   zk_scalars=None, quotient_cn=None, oods_quotient=None, quotient_tile_roots=None,
+                   oods_tile_roots=None, stream=None) -> dict:
+    """Cairo prover tail after the trace / interaction commitments
+    (cairo_air/prover.rs:1937-2438). Column arguments are lists of CUDA tensors;
+    the optional outputs are lists of 4 tensors (limbs) or one tensor (tile roots)."""
+    nt, ni = len(trace_coeffs), len(interaction_evals)
+    u64p = C.c_uint64
+    tc = (u64p * nt)(*[_ptr(t) for t in trace_coeffs])
+    te = (u64p * nt)(*[_ptr(t) for t in trace_evals])
+    ie = (u64p * max(1, ni))(*[_ptr(t) for t in interaction_evals])
+    zk = (C.c_uint32 * nt)(*[int(z) for z in zk_scalars]) if zk_scalars is not None else None
+    host = {k: (C.c_uint32 * (4 * max(1, m)))() for k, m in
+            (("trace_at_z", nt), ("trace_at_z_next", nt), ("interaction_at_z", ni), ("interaction_at_z_next", ni))}
+    io = CairoOodsFriIO()
+    io.log_n, io.n_trace, io.n_interaction = log_n, nt, ni
+    io.trace_coeffs = C.cast(tc, C.c_void_p)
+    io.trace_evals = C.cast(te, C.c_void_p)
+    io.interaction_evals = C.cast(ie, C.c_void_p)
+    io.zk_scalars = C.cast(zk, C.c_void_p) if zk is not None else None
+    for k in range(4):
+        io.quotient_hc[k] = _ptr(quotient_hc[k])
+        io.quotient_cn[k] = _ptr(quotient_cn[k]) if quotient_cn is not None else None
+        io.oods_quotient[k] = _ptr(oods_quotient[k]) if oods_quotient is not None else None
+    io.quotient_tile_roots = _ptr(quotient_tile_roots) if quotient_tile_roots is not None else None
+    io.oods_tile_roots = _ptr(oods_tile_roots) if oods_tile_roots is not None else None
+    for k, a in host.items():
+        setattr(io, k, C.cast(a, C.c_void_p))
+    check(lib().vs_cairo_oods_fri(channel.h, C.byref(io), _stream(stream)), "vs_cairo_oods_fri")
+
+    def q(arr, m):
+        return [list(arr[4 * i:4 * i + 4]) for i in range(m)]
+    return {
+        "quotient_root": list(io.quotient_root), "oods_point": list(io.oods_point),
+        "trace_at_z": q(host["trace_at_z"], nt), "trace_at_z_next": q(host["trace_at_z_next"], nt),
+        "interaction_at_z": q(host["interaction_at_z"], ni),
+        "interaction_at_z_next": q(host["interaction_at_z_next"], ni),
+        "quotient_at_z": q(io.quotient_at_z, 4), "oods_alpha": list(io.oods_alpha), "oods_root": list(io.oods_root),
+        "fri_roots": [list(io.fri_roots[8 * i:8 * i + 8]) for i in range(io.n_fri_roots)],
+        "fri_alphas": q(io.fri_alphas, log_n - 1), "last_layer": q(io.last_layer, 8),
+        "last_layer_coeffs": q(io.last_layer_coeffs, 8),
+    }

@@ -9,14 +9,19 @@
 //   permute (circle.rs:192-204) -> [coefficients] -> fused stwo LDE ->
 //   blinding with a cached Z_H (prover.rs:924-935) -> [half-coset copy
 //   (circle.rs:207-218)] -> capped-leaf root + tile roots (merkle.rs:360-417).
+#include <algorithm>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <utility>
+#include <vector>
 
+#include "fri.h"
 #include "host_math.h"
 #include "merkle.h"
 #include "ntt.h"
+#include "quotient.h"
 #include "twiddles.h"
 #include "vs_common.cuh"
 #include "vs_field.cuh"
@@ -66,6 +71,122 @@ __global__ void axpy_kernel(uint32_t r, const uint32_t* __restrict__ x, uint32_t
   if (i < n) y[i] = add(y[i], mul(r, x[i]));
 }
 
+// ------------------------------------------------------------------ evaluation at OODS points
+// A circle polynomial with stwo coefficients c_i (i < 2^L) at a QM31 point p is
+// sum_i c_i prod_{bit b of i} m_b with m_0 = p.y, m_1 = p.x, m_b = pi(m_{b-1}),
+// pi(x) = 2x^2 - 1 (oods.rs:133-161 folds the same products recursively). The
+// basis splits over the low h bits and the rest, basis_i = LO[i mod 2^h] *
+// HI[i >> h]: each thread keeps its EV_PER LO entries per point in registers and
+// walks segments of 2^h coefficients (one coalesced word per thread and entry),
+// takes the dot product of the coefficients with its LO entries per limb in 64
+// bits (folded every three products, as in the numerator kernel), reduces it,
+// multiplies by the segment's HI entry and adds it to its total. Each CTA writes
+// one partial sum per point; the host adds the partials (field addition is exact,
+// so the grouping does not change the result).
+constexpr int EV_THREADS = 256, EV_PER = 8, EV_LOG_SEG = 11;  // 2^11 = EV_THREADS * EV_PER
+constexpr int EV_MAX_POINTS = 2;
+struct EvMaps {
+  qm31 m[EV_MAX_POINTS][30];
+};
+
+// tables[p] = LO (2^h entries) then HI (2^(L-h) entries): products of the maps
+// over the set bits of the index (bits h.. for HI).
+__global__ void basis_table_kernel(EvMaps mp, uint32_t np, uint32_t h, uint32_t lo_n, uint32_t hi_n,
+                                   qm31* __restrict__ tables) {
+  const uint32_t per = lo_n + hi_n;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= np * per) return;
+  const uint32_t p = t / per, r = t % per;
+  const bool hi = r >= lo_n;
+  uint32_t idx = hi ? r - lo_n : r;
+  uint32_t b = hi ? h : 0;
+  qm31 acc{{1, 0, 0, 0}};
+  for (; idx; idx >>= 1, b++)
+    if (idx & 1) acc = qmul(acc, mp.m[p][b]);
+  tables[t] = acc;
+}
+
+__device__ __forceinline__ uint64_t ev_fold(uint64_t a) { return (a & VS_P) + (a >> 31); }
+__device__ __forceinline__ uint32_t ev_reduce(uint64_t a) { return canon((uint32_t)ev_fold(ev_fold(a))); }
+
+template <int NP>
+__global__ void __launch_bounds__(EV_THREADS) eval_points_kernel(const uint32_t* const* __restrict__ cols, uint32_t h,
+                                                                 uint32_t lo_n, uint32_t hi_n,
+                                                                 const qm31* __restrict__ tables,
+                                                                 uint32_t* __restrict__ partials) {
+  const uint32_t* col = cols[blockIdx.y];
+  const uint32_t seg = 1u << h, per = lo_n + hi_n;
+  qm31 lo[NP][EV_PER];
+#pragma unroll
+  for (int p = 0; p < NP; p++)
+#pragma unroll
+    for (int j = 0; j < EV_PER; j++) {
+      const uint32_t i = threadIdx.x + j * EV_THREADS;
+      lo[p][j] = i < seg ? tables[p * per + i] : qzero();
+    }
+  qm31 tot[NP];
+#pragma unroll
+  for (int p = 0; p < NP; p++) tot[p] = qzero();
+  for (uint32_t s = blockIdx.x; s < hi_n; s += gridDim.x) {
+    const uint32_t* base = col + (uint64_t)s * seg;
+    uint32_t x[EV_PER];
+#pragma unroll
+    for (int j = 0; j < EV_PER; j++) {
+      const uint32_t i = threadIdx.x + j * EV_THREADS;
+      x[j] = i < seg ? __ldg(base + i) : 0u;
+    }
+#pragma unroll
+    for (int p = 0; p < NP; p++) {
+      uint64_t acc[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int j = 0; j < EV_PER; j++) {
+#pragma unroll
+        for (int l = 0; l < 4; l++) acc[l] += (uint64_t)x[j] * lo[p][j].v[l];
+        if (j % 3 == 2)
+#pragma unroll
+          for (int l = 0; l < 4; l++) acc[l] = ev_fold(acc[l]);
+      }
+      qm31 part;
+#pragma unroll
+      for (int l = 0; l < 4; l++) part.v[l] = ev_reduce(acc[l]);
+      tot[p] = qadd(tot[p], qmul(part, tables[p * per + lo_n + s]));
+    }
+  }
+  __shared__ uint32_t red[EV_THREADS / 32][NP * 4];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int p = 0; p < NP; p++)
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      uint32_t v = tot[p].v[l];
+#pragma unroll
+      for (int off = 16; off; off >>= 1) v = add(v, __shfl_down_sync(0xFFFFFFFFu, v, off));
+      if (lane == 0) red[warp][p * 4 + l] = v;
+    }
+  __syncthreads();
+  if (threadIdx.x < NP * 4) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int w = 0; w < EV_THREADS / 32; w++) v = add(v, red[w][threadIdx.x]);
+    partials[((uint64_t)blockIdx.y * gridDim.x + blockIdx.x) * (NP * 4) + threadIdx.x] = v;
+  }
+}
+
+// BRT-canonic points of CanonicCoset(L): i -> j = brev_L(i); half_odds(L-1).at(j)
+// for j < 2^(L-1), its conjugate at j - 2^(L-1) otherwise (prover.rs:161-165,
+// 2213-2227). step^j = T_hi[j >> k] * T_lo[j mod 2^k] from two host-built tables,
+// so each point costs two circle multiplications.
+__global__ void canonic_points_kernel(cpt init, const cpt* __restrict__ t_lo, const cpt* __restrict__ t_hi,
+                                      uint32_t k, uint32_t L, uint32_t* __restrict__ xs, uint32_t* __restrict__ ys) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (1u << L)) return;
+  const uint32_t j = brev(i, L), half = 1u << (L - 1);
+  const uint32_t jj = j & (half - 1);
+  const cpt p = cpmul(init, cpmul(t_hi[jj >> k], t_lo[jj & ((1u << k) - 1)]));
+  xs[i] = p.x;
+  ys[i] = j >= half ? neg(p.y) : p.y;
+}
+
 namespace {
 std::mutex g_zh_mu;
 std::map<std::pair<int, uint32_t>, uint32_t*> g_zh;  // (device, log_n) -> Z_H on the 4x domain
@@ -98,6 +219,86 @@ void release_zh_tables() {
   std::lock_guard<std::mutex> lk(g_zh_mu);
   for (auto& kv : g_zh) cudaFree(kv.second);
   g_zh.clear();
+}
+
+namespace {
+// Stream-ordered allocations released (stream-ordered) when the holder goes out of scope.
+struct Scratch {
+  cudaStream_t st;
+  std::vector<void*> ptrs;
+  explicit Scratch(cudaStream_t s) : st(s) {}
+  ~Scratch() {
+    for (void* p : ptrs) cudaFreeAsync(p, st);
+  }
+  template <class T>
+  int alloc(T** out, uint64_t count) {
+    void* p = nullptr;
+    VS_CUDA(cudaMallocAsync(&p, std::max<uint64_t>(count, 1) * sizeof(T), st));
+    ptrs.push_back(p);
+    *out = static_cast<T*>(p);
+    return VS_OK;
+  }
+  // device copy of a host array (pageable source: the copy is staged before return)
+  template <class T>
+  int upload(T** out, const T* h, uint64_t count) {
+    VS_TRY(alloc(out, count));
+    VS_CUDA(cudaMemcpyAsync(*out, h, count * sizeof(T), cudaMemcpyHostToDevice, st));
+    return VS_OK;
+  }
+};
+
+h::Q pi_x(h::Q x) {  // 2x^2 - 1
+  const h::Q x2 = h::qmul(x, x);
+  return h::qsub(h::qadd(x2, x2), h::qm31_of(1));
+}
+}  // namespace
+
+// out[c * np + p] = column c (2^L stwo coefficients) at point p; synchronises st.
+int eval_at_points(const uint32_t* const* h_cols, uint32_t n_cols, uint32_t L, const h::Q (*pts)[2], uint32_t np,
+                   h::Q* out, cudaStream_t st) {
+  if (np == 0 || np > EV_MAX_POINTS) return set_error(VS_ERR_INVALID, "eval_at_points: 1 or 2 points");
+  if (L > 30) return set_error(VS_ERR_INVALID, "eval_at_points: log length %u", L);
+  if (n_cols == 0) return VS_OK;
+  if (n_cols > 65535) return set_error(VS_ERR_INVALID, "eval_at_points: too many columns");
+  EvMaps mp{};
+  for (uint32_t p = 0; p < np; p++) {
+    h::Q m = pts[p][0];  // x
+    mp.m[p][0] = qm31{{pts[p][1].v[0], pts[p][1].v[1], pts[p][1].v[2], pts[p][1].v[3]}};
+    for (uint32_t b = 1; b < L; b++) {
+      mp.m[p][b] = qm31{{m.v[0], m.v[1], m.v[2], m.v[3]}};
+      m = pi_x(m);
+    }
+  }
+  const uint32_t hb = std::min<uint32_t>(L, EV_LOG_SEG);
+  const uint32_t lo_n = 1u << hb, hi_n = 1u << (L - hb), per = lo_n + hi_n;
+  const uint32_t gx = std::max<uint32_t>(1, std::min<uint32_t>(hi_n, (uint32_t)sm_count() * 8 / n_cols));
+  Scratch s(st);
+  qm31* tables = nullptr;
+  uint32_t* partials = nullptr;
+  const uint32_t** d_cols = nullptr;
+  VS_TRY(s.alloc(&tables, (uint64_t)np * per));
+  VS_TRY(s.alloc(&partials, (uint64_t)n_cols * gx * np * 4));
+  std::vector<const uint32_t*> cols(h_cols, h_cols + n_cols);
+  VS_TRY(s.upload(&d_cols, cols.data(), n_cols));
+  basis_table_kernel<<<blocks_for((uint64_t)np * per, 256), 256, 0, st>>>(mp, np, hb, lo_n, hi_n, tables);
+  VS_LAUNCHED("basis_table_kernel");
+  const dim3 grid(gx, n_cols);
+  if (np == 1) eval_points_kernel<1><<<grid, EV_THREADS, 0, st>>>(d_cols, hb, lo_n, hi_n, tables, partials);
+  else eval_points_kernel<2><<<grid, EV_THREADS, 0, st>>>(d_cols, hb, lo_n, hi_n, tables, partials);
+  VS_LAUNCHED("eval_points_kernel");
+  std::vector<uint32_t> hp((uint64_t)n_cols * gx * np * 4);
+  VS_CUDA(cudaMemcpyAsync(hp.data(), partials, hp.size() * 4, cudaMemcpyDeviceToHost, st));
+  VS_CUDA(cudaStreamSynchronize(st));
+  for (uint32_t c = 0; c < n_cols; c++)
+    for (uint32_t p = 0; p < np; p++) {
+      h::Q acc{{0, 0, 0, 0}};
+      for (uint32_t b = 0; b < gx; b++) {
+        const uint32_t* v = &hp[(((uint64_t)c * gx + b) * np + p) * 4];
+        acc = h::qadd(acc, h::Q{{v[0], v[1], v[2], v[3]}});
+      }
+      out[c * np + p] = acc;
+    }
+  return VS_OK;
 }
 
 }  // namespace vs
@@ -171,4 +372,326 @@ extern "C" int vs_commit_group_cairo(const uint32_t* d_cols_hc, uint64_t col_str
     }
   }
   return rc;
+}
+
+extern "C" int vs_eval_at_oods_points(const uint32_t* const* h_cols, uint32_t n_cols, uint32_t log_len,
+                                      const uint32_t* h_points, uint32_t n_points, uint32_t* h_out,
+                                      vs_stream_t stream) {
+  clear_error();
+  if (!h_points || (n_cols && (!h_cols || !h_out))) return set_error(VS_ERR_INVALID, "vs_eval_at_oods_points: null");
+  if (n_points == 0 || n_points > EV_MAX_POINTS) return set_error(VS_ERR_INVALID, "vs_eval_at_oods_points: 1 or 2 points");
+  for (uint32_t c = 0; c < n_cols; c++)
+    if (!h_cols[c]) return set_error(VS_ERR_INVALID, "vs_eval_at_oods_points: null column %u", c);
+  h::Q pts[EV_MAX_POINTS][2];
+  for (uint32_t p = 0; p < n_points; p++)
+    for (int l = 0; l < 4; l++) {
+      pts[p][0].v[l] = h_points[8 * p + l];
+      pts[p][1].v[l] = h_points[8 * p + 4 + l];
+      if (pts[p][0].v[l] >= VS_P || pts[p][1].v[l] >= VS_P)
+        return set_error(VS_ERR_INVALID, "vs_eval_at_oods_points: point not canonical");
+    }
+  std::vector<h::Q> out((uint64_t)n_cols * n_points);
+  VS_TRY(eval_at_points(h_cols, n_cols, log_len, pts, n_points, out.data(), (cudaStream_t)stream));
+  for (uint64_t i = 0; i < out.size(); i++) std::memcpy(h_out + 4 * i, out[i].v, 16);
+  return VS_OK;
+}
+
+namespace {
+// SoA4 commitment with 1024-leaf tile roots (merkle.rs:294-330): the root alone
+// (copied into tiles) below 1024 leaves.
+int commit_soa4_tiles(uint32_t* const c[4], uint64_t N, uint32_t* d_root, uint32_t* tiles, cudaStream_t st) {
+  const LeafSoa4 leaf{c[0], c[1], c[2], c[3]};
+  if (N < 1024) {
+    VS_TRY(merkle_root(leaf, N, d_root, st));
+    VS_CUDA(cudaMemcpyAsync(tiles, d_root, 32, cudaMemcpyDeviceToDevice, st));
+    return VS_OK;
+  }
+  VS_TRY(merkle_tile_roots(leaf, N, 10, tiles, st));
+  return merkle_root(LeafHashes{tiles}, N / 1024, d_root, st);
+}
+int read_hash(const uint32_t* d, h::Hash& out, cudaStream_t st) {
+  VS_CUDA(cudaMemcpyAsync(out.data(), d, 32, cudaMemcpyDeviceToHost, st));
+  VS_CUDA(cudaStreamSynchronize(st));
+  return VS_OK;
+}
+// fri.rs:294-336: 8 BRT-ordered line evaluations on half_odds(3) -> natural
+// coefficients (bit-reverse, line iFFT with 1/x twiddles, scale by 1/n, bit-reverse)
+std::vector<h::Q> line_coeffs_from_evals(std::vector<h::Q> e) {
+  const uint32_t n = (uint32_t)e.size(), lg = ilog2(n);
+  auto brev_all = [&](std::vector<h::Q>& v) {
+    for (uint32_t i = 0; i < n; i++) {
+      const uint32_t j = (uint32_t)h::brev(i, lg);
+      if (i < j) std::swap(v[i], v[j]);
+    }
+  };
+  brev_all(e);
+  for (uint32_t chunk = n, dl = lg; chunk > 1; chunk >>= 1, dl--) {
+    const h::Coset dom = h::half_odds(dl);
+    const uint32_t half = chunk / 2;
+    for (uint32_t base = 0; base < n; base += chunk)
+      for (uint32_t i = 0; i < half; i++) {
+        const uint32_t xi = h::inv(dom.at(i).x);
+        const h::Q l = e[base + i], r = e[base + half + i];
+        e[base + i] = h::qadd(l, r);
+        e[base + half + i] = h::qscale(h::qsub(l, r), xi);
+      }
+  }
+  const uint32_t ninv = h::inv(n);
+  for (auto& v : e) v = h::qscale(v, ninv);
+  brev_all(e);
+  return e;
+}
+void put_q(uint32_t* dst, const h::Q& q) { std::memcpy(dst, q.v, 16); }
+}  // namespace
+
+extern "C" int vs_cairo_oods_fri(void* channel, vs_cairo_oods_fri_io* io, vs_stream_t stream) {
+  clear_error();
+  auto* ch = static_cast<h::Channel*>(channel);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!ch || !io) return set_error(VS_ERR_INVALID, "vs_cairo_oods_fri: null argument");
+  const uint32_t log_n = io->log_n, nt = io->n_trace, ni = io->n_interaction;
+  if (log_n < 2 || log_n > 26) return set_error(VS_ERR_INVALID, "vs_cairo_oods_fri: log_n %u outside [2, 26]", log_n);
+  if (nt == 0 || nt > 1024 || ni > 1024) return set_error(VS_ERR_INVALID, "vs_cairo_oods_fri: column counts");
+  if (!io->trace_coeffs || !io->trace_evals || (ni && !io->interaction_evals))
+    return set_error(VS_ERR_INVALID, "vs_cairo_oods_fri: null column table");
+  for (uint32_t c = 0; c < nt; c++) {
+    if (!io->trace_coeffs[c] || !io->trace_evals[c]) return set_error(VS_ERR_INVALID, "vs_cairo_oods_fri: null trace column");
+    if (io->zk_scalars && io->zk_scalars[c] >= VS_P) return set_error(VS_ERR_INVALID, "vs_cairo_oods_fri: blinding scalar");
+  }
+  for (uint32_t c = 0; c < ni; c++)
+    if (!io->interaction_evals[c]) return set_error(VS_ERR_INVALID, "vs_cairo_oods_fri: null interaction column");
+  for (int k = 0; k < 4; k++)
+    if (!io->quotient_hc[k]) return set_error(VS_ERR_INVALID, "vs_cairo_oods_fri: null quotient limb");
+  const uint32_t log_eval = log_n + 2;
+  const uint64_t N = 1ull << log_eval;
+  const uint64_t n_tiles = N < 1024 ? 1 : N / 1024;
+  Scratch s(st);
+  uint32_t* d_root = nullptr;
+  VS_TRY(s.alloc(&d_root, 8));
+  h::Hash root;
+
+  // AIR quotient: half-coset natural -> BRT-canonic, SoA4 commitment (prover.rs:1937-1971)
+  uint32_t* qcn[4];
+  for (int k = 0; k < 4; k++) {
+    qcn[k] = io->quotient_cn[k];
+    if (!qcn[k]) VS_TRY(s.alloc(&qcn[k], N));
+    permute_kernel<true><<<dim3(blocks_for(N, 256), 1), 256, 0, st>>>(io->quotient_hc[k], N, qcn[k], N, log_eval);
+    VS_LAUNCHED("permute_kernel");
+  }
+  uint32_t* qtiles = io->quotient_tile_roots;
+  if (!qtiles) VS_TRY(s.alloc(&qtiles, n_tiles * 8));
+  VS_TRY(commit_soa4_tiles(qcn, N, d_root, qtiles, st));
+  VS_TRY(read_hash(d_root, root, st));
+  std::memcpy(io->quotient_root, root.data(), 32);
+  ch->mix_digest(root);
+
+  // OODS point z and z_next = z + one trace step (oods.rs:44-81; prover.rs:1978-1984)
+  const h::Q t = ch->draw_felt(), one = h::qm31_of(1);
+  const h::Q t2 = h::qmul(t, t), di = h::qinv(h::qadd(one, t2));
+  const h::Q zx = h::qmul(h::qsub(one, t2), di), zy = h::qmul(h::qadd(t, t), di);
+  h::Pt step{2, 1268011823u};
+  for (uint32_t i = 0; i < 31 - log_n; i++) step = h::pmul(step, step);
+  const h::Q nx = h::qsub(h::qscale(zx, step.x), h::qscale(zy, step.y));
+  const h::Q ny = h::qadd(h::qscale(zx, step.y), h::qscale(zy, step.x));
+  h::Q zh_z = zx, zh_n = nx;  // oods.rs:285-291
+  for (uint32_t i = 1; i < log_n; i++) { zh_z = pi_x(zh_z); zh_n = pi_x(zh_n); }
+  const h::Q pts[2][2] = {{zx, zy}, {nx, ny}};
+
+  // trace columns at z and z_next from their coefficients, plus r * Z_H (prover.rs:1987-2001)
+  std::vector<h::Q> tv(2 * nt), iv(2 * ni);
+  VS_TRY(eval_at_points(io->trace_coeffs, nt, log_n, pts, 2, tv.data(), st));
+  if (io->zk_scalars)
+    for (uint32_t c = 0; c < nt; c++)
+      if (const uint32_t r = io->zk_scalars[c]) {
+        tv[2 * c] = h::qadd(tv[2 * c], h::qscale(zh_z, r));
+        tv[2 * c + 1] = h::qadd(tv[2 * c + 1], h::qscale(zh_n, r));
+      }
+  // interaction columns: first 2^log_n stwo coefficients of their evaluations (prover.rs:2037-2048)
+  NttTw ti;
+  VS_TRY(tw_for(TW_STWO, log_eval, false, &ti, st));
+  const uint32_t B = std::min<uint32_t>(std::max<uint32_t>(ni, 4), 8);
+  uint32_t* coef = nullptr;
+  VS_TRY(s.alloc(&coef, B * N));
+  std::vector<const uint32_t*> cp(B);
+  for (uint32_t j = 0; j < B; j++) cp[j] = coef + j * N;
+  for (uint32_t c0 = 0; c0 < ni; c0 += B) {
+    const uint32_t nb = std::min(B, ni - c0);
+    for (uint32_t j = 0; j < nb; j++)
+      VS_CUDA(cudaMemcpyAsync(coef + j * N, io->interaction_evals[c0 + j], N * 4, cudaMemcpyDeviceToDevice, st));
+    VS_TRY(ntt_transform(NttColumns{coef, coef, nullptr, nullptr, N, N, nb}, log_eval, ti, false, st));
+    VS_TRY(eval_at_points(cp.data(), nb, log_n, pts, 2, iv.data() + 2 * c0, st));
+  }
+  // quotient limbs at z from all their coefficients (prover.rs:2053-2065)
+  h::Q qv[4];
+  for (int k = 0; k < 4; k++)
+    VS_CUDA(cudaMemcpyAsync(coef + k * N, qcn[k], N * 4, cudaMemcpyDeviceToDevice, st));
+  VS_TRY(ntt_transform(NttColumns{coef, coef, nullptr, nullptr, N, N, 4}, log_eval, ti, false, st));
+  VS_TRY(eval_at_points(cp.data(), 4, log_eval, pts, 1, qv, st));
+
+  // sampled values in flatten_cols order, then the OODS alpha (prover.rs:2067-2095)
+  {
+    std::vector<h::Q> all;
+    all.reserve(2 * nt + 2 * ni + 4);
+    for (uint32_t c = 0; c < nt; c++) { all.push_back(tv[2 * c]); all.push_back(tv[2 * c + 1]); }
+    for (uint32_t c = 0; c < ni; c++) { all.push_back(iv[2 * c]); all.push_back(iv[2 * c + 1]); }
+    for (int k = 0; k < 4; k++) all.push_back(qv[k]);
+    ch->mix_felts(all);
+  }
+  const h::Q alpha = ch->draw_felt();
+
+  // alpha-weighted line coefficients (prover.rs:2095-2150; oods.rs compute_line_coeffs)
+  std::vector<uint32_t> bz, cz, bn, cn;
+  h::Q lin_z{{0, 0, 0, 0}}, lin_n{{0, 0, 0, 0}}, ap = one;
+  auto push = [&](const h::Q& py, const h::Q& v, std::vector<uint32_t>& bv, std::vector<uint32_t>& cv, h::Q& lin) {
+    const h::Q b = h::qmul(h::qsub(v, h::qconj(v)), h::qinv(h::qsub(py, h::qconj(py))));
+    const h::Q a = h::qsub(v, h::qmul(b, py));
+    const h::Q wa = h::qmul(ap, a);
+    bv.insert(bv.end(), wa.v, wa.v + 4);
+    cv.insert(cv.end(), ap.v, ap.v + 4);
+    lin = h::qadd(lin, h::qmul(ap, b));
+    ap = h::qmul(ap, alpha);
+  };
+  for (uint32_t c = 0; c < nt; c++) push(zy, tv[2 * c], bz, cz, lin_z);
+  for (int k = 0; k < 4; k++) push(zy, qv[k], bz, cz, lin_z);
+  for (uint32_t c = 0; c < ni; c++) push(zy, iv[2 * c], bz, cz, lin_z);
+  for (uint32_t c = 0; c < nt; c++) push(ny, tv[2 * c + 1], bn, cn, lin_n);
+  for (uint32_t c = 0; c < ni; c++) push(ny, iv[2 * c + 1], bn, cn, lin_n);
+
+  // DEEP numerators over [trace, quotient, interaction] (prover.rs:2152-2207)
+  const uint32_t n_all = nt + 4 + ni;
+  std::vector<const uint32_t*> cols;
+  cols.reserve(n_all);
+  for (uint32_t c = 0; c < nt; c++) cols.push_back(io->trace_evals[c]);
+  for (int k = 0; k < 4; k++) cols.push_back(qcn[k]);
+  for (uint32_t c = 0; c < ni; c++) cols.push_back(io->interaction_evals[c]);
+  bool vec = N % 4 == 0;
+  for (const uint32_t* p : cols) vec = vec && (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+  std::vector<uint32_t> idx_z(n_all), idx_n;
+  for (uint32_t i = 0; i < n_all; i++) idx_z[i] = i;
+  for (uint32_t i = 0; i < nt; i++) idx_n.push_back(i);
+  for (uint32_t i = 0; i < ni; i++) idx_n.push_back(nt + 4 + i);
+  const uint32_t** d_cols = nullptr;
+  uint32_t *d_iz, *d_in, *d_bz, *d_cz, *d_bn, *d_cn, *numer;
+  VS_TRY(s.upload(&d_cols, cols.data(), n_all));
+  VS_TRY(s.upload(&d_iz, idx_z.data(), idx_z.size()));
+  VS_TRY(s.upload(&d_in, idx_n.data(), idx_n.size()));
+  VS_TRY(s.upload(&d_bz, bz.data(), bz.size()));
+  VS_TRY(s.upload(&d_cz, cz.data(), cz.size()));
+  VS_TRY(s.upload(&d_bn, bn.data(), bn.size()));
+  VS_TRY(s.upload(&d_cn, cn.data(), cn.size()));
+  VS_TRY(s.alloc(&numer, 8 * N));
+  uint32_t* const num_z[4] = {numer, numer + N, numer + 2 * N, numer + 3 * N};
+  uint32_t* const num_n[4] = {numer + 4 * N, numer + 5 * N, numer + 6 * N, numer + 7 * N};
+  VS_TRY(launch_accumulate_numerators(d_cols, d_iz, d_bz, d_cz, n_all, (uint32_t)N, num_z, vec, st));
+  VS_TRY(launch_accumulate_numerators(d_cols, d_in, d_bn, d_cn, nt + ni, (uint32_t)N, num_n, vec, st));
+
+  // BRT-canonic domain points and the combination (prover.rs:2213-2266)
+  uint32_t *xs, *ys;
+  VS_TRY(s.alloc(&xs, N));
+  VS_TRY(s.alloc(&ys, N));
+  {
+    const h::Coset ho = h::half_odds(log_eval - 1);
+    const uint32_t k = (log_eval - 1) / 2;
+    std::vector<cpt> tlo(1u << k), thi(1u << (log_eval - 1 - k));
+    h::Pt a{1, 0};
+    for (auto& e : tlo) { e = cpt{a.x, a.y}; a = h::pmul(a, ho.step); }
+    const h::Pt big = h::ppow(ho.step, 1ull << k);
+    a = h::Pt{1, 0};
+    for (auto& e : thi) { e = cpt{a.x, a.y}; a = h::pmul(a, big); }
+    cpt *d_lo, *d_hi;
+    VS_TRY(s.upload(&d_lo, tlo.data(), tlo.size()));
+    VS_TRY(s.upload(&d_hi, thi.data(), thi.size()));
+    canonic_points_kernel<<<blocks_for(N, 256), 256, 0, st>>>(cpt{ho.initial.x, ho.initial.y}, d_lo, d_hi, k,
+                                                              log_eval, xs, ys);
+    VS_LAUNCHED("canonic_points_kernel");
+  }
+  uint32_t meta[4 * 2 * 3 + 2];  // spx[8] spy[8] fla[8] acc_log[2]
+  std::memcpy(meta, zx.v, 16);
+  std::memcpy(meta + 4, nx.v, 16);
+  std::memcpy(meta + 8, zy.v, 16);
+  std::memcpy(meta + 12, ny.v, 16);
+  std::memcpy(meta + 16, lin_z.v, 16);
+  std::memcpy(meta + 20, lin_n.v, 16);
+  meta[24] = meta[25] = log_eval;
+  const uint32_t* nptr[8] = {num_z[0], num_n[0], num_z[1], num_n[1], num_z[2], num_n[2], num_z[3], num_n[3]};
+  uint32_t* d_meta;
+  const uint32_t** d_np;
+  VS_TRY(s.upload(&d_meta, meta, 26));
+  VS_TRY(s.upload(&d_np, nptr, 8));
+  uint32_t* oq[4];
+  for (int k = 0; k < 4; k++) {
+    oq[k] = io->oods_quotient[k];
+    if (!oq[k]) VS_TRY(s.alloc(&oq[k], N));
+  }
+  VS_TRY(launch_quotients_combine(d_meta, d_meta + 8, d_meta + 16, d_np, d_np + 2, d_np + 4, d_np + 6, d_meta + 24, 2,
+                                  xs, ys, log_eval, (uint32_t)N, oq, st));
+  uint32_t* otiles = io->oods_tile_roots;
+  if (!otiles) VS_TRY(s.alloc(&otiles, n_tiles * 8));
+  VS_TRY(commit_soa4_tiles(oq, N, d_root, otiles, st));
+  VS_TRY(read_hash(d_root, root, st));
+  std::memcpy(io->oods_root, root.data(), 32);
+  ch->mix_digest(root);
+
+  // FRI: circle fold with 1/y of the canonic points, then committed line folds
+  // down to 8 values; each fold is fused with the commitment of its output
+  // (prover.rs:2321-2381)
+  uint32_t* fri = nullptr;
+  VS_TRY(s.alloc(&fri, 4 * N));
+  uint32_t* src[4] = {oq[0], oq[1], oq[2], oq[3]};
+  uint32_t* dst[4];
+  uint64_t off = 0;
+  h::Q fa = ch->draw_felt();
+  std::vector<h::Q> alphas{fa};
+  std::vector<h::Hash> roots;
+  const uint32_t* tw = nullptr;
+  VS_TRY(get_fold_twiddles(FOLD_CANONIC_CIRCLE, log_eval, &tw, st));
+  uint64_t half = N / 2;
+  for (int k = 0; k < 4; k++) dst[k] = fri + off + k * half;
+  off += 4 * half;
+  VS_TRY(fold_commit_layer(src, dst, tw, fa.v, nullptr, false, half, d_root, nullptr, st));
+  for (uint32_t cur = log_eval - 1; cur > 3; cur--) {
+    VS_TRY(read_hash(d_root, root, st));
+    ch->mix_digest(root);
+    roots.push_back(root);
+    fa = ch->draw_felt();
+    alphas.push_back(fa);
+    VS_TRY(get_fold_twiddles(COSET_HALF_ODDS, cur, &tw, st));
+    for (int k = 0; k < 4; k++) src[k] = dst[k];
+    half >>= 1;
+    for (int k = 0; k < 4; k++) dst[k] = fri + off + k * half;
+    off += 4 * half;
+    VS_TRY(fold_commit_layer(src, dst, tw, fa.v, nullptr, false, half, d_root, nullptr, st));
+  }
+  std::vector<uint32_t> planes(32);
+  for (int k = 0; k < 4; k++)
+    VS_CUDA(cudaMemcpyAsync(planes.data() + 8 * k, dst[k], 32, cudaMemcpyDeviceToHost, st));
+  VS_CUDA(cudaStreamSynchronize(st));
+  std::vector<h::Q> last(8);
+  for (int i = 0; i < 8; i++) last[i] = h::Q{{planes[i], planes[8 + i], planes[16 + i], planes[24 + i]}};
+  const std::vector<h::Q> nat = line_coeffs_from_evals(last);
+  std::vector<h::Q> brt(8);
+  for (uint32_t i = 0; i < 8; i++) brt[h::brev(i, 3)] = nat[i];
+  ch->mix_felts(brt);
+
+  // results
+  for (uint32_t c = 0; c < nt; c++) {
+    if (io->trace_at_z) put_q(io->trace_at_z + 4 * c, tv[2 * c]);
+    if (io->trace_at_z_next) put_q(io->trace_at_z_next + 4 * c, tv[2 * c + 1]);
+  }
+  for (uint32_t c = 0; c < ni; c++) {
+    if (io->interaction_at_z) put_q(io->interaction_at_z + 4 * c, iv[2 * c]);
+    if (io->interaction_at_z_next) put_q(io->interaction_at_z_next + 4 * c, iv[2 * c + 1]);
+  }
+  put_q(io->oods_point, zx);
+  put_q(io->oods_point + 4, zy);
+  for (int k = 0; k < 4; k++) put_q(io->quotient_at_z + 4 * k, qv[k]);
+  put_q(io->oods_alpha, alpha);
+  io->n_fri_roots = (uint32_t)roots.size();
+  for (size_t i = 0; i < roots.size(); i++) std::memcpy(io->fri_roots + 8 * i, roots[i].data(), 32);
+  for (size_t i = 0; i < alphas.size(); i++) put_q(io->fri_alphas + 4 * i, alphas[i]);
+  for (int i = 0; i < 8; i++) {
+    put_q(io->last_layer + 4 * i, last[i]);
+    put_q(io->last_layer_coeffs + 4 * i, brt[i]);
+  }
+  return VS_OK;
 }

@@ -47,6 +47,26 @@ inline Q qmul(Q x, Q y) {
   return {{add(acr, ur), add(aci, ui), add(adr, bcr), add(adi, bci)}};
 }
 
+inline Q qconj(Q x) { return {{x.v[0], x.v[1], neg(x.v[2]), neg(x.v[3])}}; }  // a + bu -> a - bu
+// (a + bu)^-1 = (a - bu) / (a^2 - (2 + i) b^2), the denominator inverted in CM31
+// as conj(d) / |d|^2 (qm31.rs inverse). Zero maps to zero.
+inline Q qinv(Q x) {
+  const uint32_t a2r = sub(mul(x.v[0], x.v[0]), mul(x.v[1], x.v[1])), a2i = dbl(mul(x.v[0], x.v[1]));
+  const uint32_t b2r = sub(mul(x.v[2], x.v[2]), mul(x.v[3], x.v[3])), b2i = dbl(mul(x.v[2], x.v[3]));
+  const uint32_t dr = sub(a2r, sub(dbl(b2r), b2i)), di = sub(a2i, add(b2r, dbl(b2i)));
+  const uint32_t s = inv(add(mul(dr, dr), mul(di, di)));
+  const uint32_t ir = mul(dr, s), ii = mul(neg(di), s);
+  auto cm = [](uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t& re, uint32_t& im) {
+    re = sub(mul(a, c), mul(b, d));
+    im = add(mul(a, d), mul(b, c));
+  };
+  Q r;
+  cm(x.v[0], x.v[1], ir, ii, r.v[0], r.v[1]);
+  cm(neg(x.v[2]), neg(x.v[3]), ir, ii, r.v[2], r.v[3]);
+  return r;
+}
+inline Q qm31_of(uint32_t a) { return {{a, 0, 0, 0}}; }
+
 struct Pt { uint32_t x, y; };
 inline Pt pmul(Pt a, Pt b) { return {sub(mul(a.x, b.x), mul(a.y, b.y)), add(mul(a.x, b.y), mul(a.y, b.x))}; }
 inline Pt ppow(Pt b, uint64_t e) {

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "quotient.h"
 #include "vs_common.cuh"
 #include "vs_field.cuh"
 #include "vs_mem.cuh"
@@ -230,6 +231,32 @@ __global__ void fill_uniform_kernel(uint32_t* __restrict__ out, uint64_t n, uint
     }
     out[i] = v;
   }
+}
+
+int launch_accumulate_numerators(const uint32_t* const* d_cols, const uint32_t* d_idx, const uint32_t* d_b,
+                                 const uint32_t* d_c, uint32_t n_batch, uint32_t n_rows, uint32_t* const o[4],
+                                 bool vec, cudaStream_t st) {
+  if (!n_rows) return VS_OK;
+  const unsigned blocks = blocks_for((n_rows + AN_ROWS - 1) / AN_ROWS, 256);
+  if (vec)
+    accumulate_numerators_kernel<true><<<blocks, 256, 0, st>>>(d_cols, d_idx, d_b, d_c, n_batch, n_rows, o[0], o[1],
+                                                               o[2], o[3]);
+  else
+    accumulate_numerators_kernel<false><<<blocks, 256, 0, st>>>(d_cols, d_idx, d_b, d_c, n_batch, n_rows, o[0], o[1],
+                                                                o[2], o[3]);
+  VS_LAUNCHED("accumulate_numerators_kernel");
+  return VS_OK;
+}
+int launch_quotients_combine(const uint32_t* spx, const uint32_t* spy, const uint32_t* fla,
+                             const uint32_t* const* n0, const uint32_t* const* n1, const uint32_t* const* n2,
+                             const uint32_t* const* n3, const uint32_t* acc_log, uint32_t n_accs,
+                             const uint32_t* dxs, const uint32_t* dys, uint32_t lifting_log, uint32_t n_rows,
+                             uint32_t* const o[4], cudaStream_t st) {
+  if (!n_rows) return VS_OK;
+  quotients_combine_kernel<<<blocks_for((n_rows + QC_ROWS - 1) / QC_ROWS, 256), 256, 0, st>>>(
+      spx, spy, fla, n0, n1, n2, n3, acc_log, n_accs, dxs, dys, lifting_log, n_rows, o[0], o[1], o[2], o[3]);
+  VS_LAUNCHED("quotients_combine_kernel");
+  return VS_OK;
 }
 
 }  // namespace vs

@@ -263,10 +263,13 @@ int get_fold_twiddles(int which, uint32_t log_n, const uint32_t** out, cudaStrea
   t->log_n = log_n;
   const uint32_t half = 1u << (log_n - 1);
   if (cudaMalloc(&t->mem, (size_t)half * 2 * 4) != cudaSuccess) { delete t; return set_error(VS_ERR_OOM, "fold twiddles: alloc"); }
-  HostCoset c = host_coset(which, log_n);
+  HostCoset c = host_coset(which == FOLD_CANONIC_CIRCLE ? COSET_HALF_COSET : which, log_n);
+  // half_odds(L-1) has half_coset(L)'s initial point and twice its step; with the
+  // L-bit reversal of 2i this gives half_odds(L-1).at(brev_{L-1}(i)).
+  if (which == FOLD_CANONIC_CIRCLE) c.step = host_mul(c.step, c.step);
   uint32_t* src = t->mem + half;
   fold_sources_kernel<<<blocks_for(half, 256), 256, 0, st>>>(c.initial, c.step, src, half, log_n,
-                                                             which == COSET_HALF_COSET ? 1 : 0);
+                                                             (which == COSET_HALF_COSET || which == FOLD_CANONIC_CIRCLE) ? 1 : 0);
   VS_LAUNCHED("fold_sources_kernel");
   t->line = t->mem;
   VS_TRY(launch_batch_inverse(src, t->line, half, st));

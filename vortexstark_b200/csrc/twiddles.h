@@ -11,6 +11,9 @@ namespace vs {
 
 enum { TW_NATIVE = 0, TW_STWO = 1 };
 enum { COSET_HALF_COSET = 0, COSET_HALF_ODDS = 1, COSET_SUBGROUP = 2 };
+// Fold twiddles only: the circle fold of a BRT-canonic evaluation on
+// CanonicCoset(L), 1/y(half_odds(L-1).at(brev_{L-1}(i))) (cairo_air/prover.rs:2327-2335).
+enum { FOLD_CANONIC_CIRCLE = 3 };
 
 struct TwiddleSet {
   int kind = 0;
@@ -36,7 +39,8 @@ cpt host_repeated_double(cpt p, uint32_t k);
 // Cached per (device, kind, log_n); built on the device on first use.
 int get_twiddles(int kind, uint32_t log_n, const TwiddleSet** out, cudaStream_t st);
 // FRI fold twiddles 1/coord(domain.at(bitrev(2i))) for the coset `which`
-// (half_coset -> y, half_odds -> x), cached per (device, which, log_n).
+// (half_coset -> y, half_odds -> x, FOLD_CANONIC_CIRCLE -> y), cached per
+// (device, which, log_n).
 int get_fold_twiddles(int which, uint32_t log_n, const uint32_t** out, cudaStream_t st);
 int release_twiddles();
 // Frees the cached vanishing-polynomial tables of the Cairo group commit (cairo.cu).
