@@ -19,6 +19,7 @@ data path); rank 0 prints one JSON line.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -37,6 +38,7 @@ sys.path.insert(0, str(ROOT))
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 SEED = 0x56530001
+P = 0x7FFFFFFF
 METRIC = "committed M31 elems/s & proofs/s batched vs plain on 1 B200; p50/p99 latency"
 UNIT = "committed M31 elements/s"
 
@@ -228,6 +230,83 @@ def oods_quotients(args, V, torch, lde, N, st, ev):
     return res
 
 
+# ---------------------------------------------------------------- Cairo trace chain
+def cairo_chain(args, V, torch, ev):
+    """The reference Cairo prover's commitment chain at production width, on the
+    device: 34 trace columns (half-coset order) committed as groups 16 / 15 / 3
+    with coefficients, blinding, half-coset copies and tile roots
+    (cairo_air/prover.rs:899-1047), then the tail from the AIR-quotient commitment
+    through OODS, the DEEP quotient and FRI (prover.rs:1937-2438) with 12
+    interaction columns. Seeded inputs; the AIR quotient is a seeded polynomial of
+    degree < 2n (the constraint evaluation itself is Cairo-specific and not on this
+    path). CUDA-event time on the current stream."""
+    from vortexstark_b200 import api
+    log_n = args.cairo_log_n
+    n, N = 1 << log_n, 4 << log_n
+    dev = torch.device("cuda")
+    mk = lambda *s: torch.empty(s, dtype=torch.int32, device=dev)  # noqa: E731
+    cols = api.fill_uniform_m31(mk(34, n), SEED + 20)
+    blind = [(SEED * 7919 + 104729 * c) % P for c in range(34)]
+    coeffs, evals, evals_hc = mk(34, n), mk(34, N), mk(34, N)
+    tiles = [mk(max(1, N // 1024) * 8) for _ in range(3)]
+    groups = ((0, 16), (16, 31), (31, 34))
+    inter = api.lde_stwo(api.fill_uniform_m31(mk(12, n), SEED + 21), log_n, 2)
+    q_cn = api.lde_stwo(api.fill_uniform_m31(mk(4, 2 * n), SEED + 22), log_n + 1, 1)
+    k = torch.arange(N, dtype=torch.int64, device=dev)
+    cn = torch.where(k % 2 == 0, k // 2, N - 1 - k // 2)
+    pos = torch.zeros_like(cn)
+    for b in range(log_n + 2):
+        pos |= ((cn >> b) & 1) << (log_n + 1 - b)
+    q_hc = q_cn[:, pos].contiguous()
+    del k, cn, pos
+    L = V.lib()
+    st = torch.cuda.current_stream()
+
+    def commit():
+        roots = []
+        for g, (a, b) in enumerate(groups):
+            root = mk(8)
+            V.check(L.vs_commit_group_cairo(cols[a].data_ptr(), n, b - a, log_n, (C.c_uint32 * (b - a))(*blind[a:b]),
+                                            coeffs[a].data_ptr(), evals[a].data_ptr(), evals_hc[a].data_ptr(),
+                                            root.data_ptr(), tiles[g].data_ptr(), st.cuda_stream),
+                    "vs_commit_group_cairo")
+            roots.append(root)
+        return roots
+
+    def tail(roots):
+        ch = api.Channel()
+        for r in roots:
+            ch.mix_digest(r.cpu().numpy().view("uint32"))
+        return api.cairo_oods_fri(ch, log_n, list(coeffs), list(evals), list(inter), list(q_hc), zk_scalars=blind)
+
+    tail(commit())
+    torch.cuda.synchronize()
+    t_commit, t_tail = [], []
+    low_degree = True
+    iters = max(1, args.steps // 2)
+    c0 = api.launch_count()
+    for _ in range(iters):
+        e0, e1, e2 = ev(), ev(), ev()
+        e0.record(st)
+        roots = commit()
+        e1.record(st)
+        r = tail(roots)
+        e2.record(st)
+        torch.cuda.synchronize()
+        t_commit.append(e0.elapsed_time(e1))
+        t_tail.append(e1.elapsed_time(e2))
+        nat = [r["last_layer_coeffs"][i] for i in (0, 4, 2, 6, 1, 5, 3, 7)]
+        low_degree = low_degree and not any(any(c) for c in nat[4:])
+    res = {"workload": f"34 trace columns (16/15/3) x 2^{log_n} rows, x4 LDE; 12 interaction columns; "
+                       "AIR quotient of degree < 2n", "log_n": log_n,
+           "commit_ms": statistics.median(t_commit), "tail_ms": statistics.median(t_tail),
+           "trace_elements_committed": 34 * N, "last_layer_low_degree": low_degree,
+           "gpu_launches_per_chain": (api.launch_count() - c0) // iters}
+    del cols, coeffs, evals, evals_hc, inter, q_cn, q_hc
+    torch.cuda.empty_cache()
+    return res
+
+
 # ---------------------------------------------------------------- proof workloads
 def proof_workloads(args):
     """Proof throughput and latency. The plain path is the drop-in single-job
@@ -242,9 +321,6 @@ def proof_workloads(args):
             eng.prepare(api.commit_job(j.log_n, 34, 0) if j.kind == api.COMMIT else j)
 
     out = {}
-    # the stream-ordered pool keeps what it has allocated, as the reference's own
-    # benchmark sets it (init_memory_pool_greedy, src/bin/full_benchmark.rs:23)
-    api.init_memory_pool((1 << 64) - 1)
     plain = W.plain_jobs(64, 16)
     W.run_plain(plain[:4])
     t_plain, r_plain = W.run_plain(plain)
@@ -332,6 +408,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-proofs", action="store_true", help="skip the plain / batched / served proof runs")
     ap.add_argument("--no-oods", action="store_true", help="skip the OODS quotient kernels")
+    ap.add_argument("--no-cairo", action="store_true", help="skip the Cairo trace commitment + tail chain")
+    ap.add_argument("--cairo-log-n", type=int, default=22, help="trace rows (log) of the Cairo chain")
     ap.add_argument("--slots", type=int, default=8, help="concurrent slots of the batched and served engines")
     ap.add_argument("--served-jobs", type=int, default=600)
     ap.add_argument("--prove-sizes", type=int, nargs="*", default=[20, 24, 28],
@@ -353,6 +431,9 @@ def main():
     os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
     replicas.init("nccl", timeout_s=120)
     V.lib()  # raises if the CUDA library is missing
+    # The stream-ordered pool keeps what it has allocated, as the reference's own
+    # benchmark sets it (init_memory_pool_greedy, src/bin/full_benchmark.rs:23).
+    api.init_memory_pool((1 << 64) - 1)
 
     n_cols, log_n, blow, fri_log, N, committed = workload(args)
     n = 1 << log_n
@@ -512,11 +593,14 @@ def main():
             "launch_ms": phase["merkle"], "phase_ms": phase,
             "phase_hbm_frac": {k: alg[k] / (phase[k] / 1e3) / 1e9 / hbm for k in phase}}
 
-    proofs = None
-    if rank == 0 and world == 1 and not args.no_proofs:
+    proofs = cairo = None
+    if rank == 0 and world == 1 and not (args.no_proofs and args.no_cairo):
         del lde, cols, fri_src, work
         torch.cuda.empty_cache()
-        proofs = proof_workloads(args)
+        if not args.no_cairo:
+            cairo = cairo_chain(args, V, torch, ev)
+        if not args.no_proofs:
+            proofs = proof_workloads(args)
     if rank == 0:
         cpu = None if args.no_cpu else cpu_sample(args, os.cpu_count() or 1)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -524,7 +608,7 @@ def main():
                 "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic (seeded SplitMix64 uniform M31)",
                 "config": config_json(args), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clk.summary(), "three_tree_commit": three, "oods": oods,
-                "proofs": proofs}
+                "cairo": cairo, "proofs": proofs}
         print(json.dumps(line), flush=True)
     replicas.finalize()
 
