@@ -63,13 +63,23 @@ def test_group_commit_matches_oracle(L, log_n, nc):
     check(run_group(L, cols, log_n, blind), O.commit_group_cairo(cols, log_n, blind))
 
 
-@pytest.mark.parametrize("log_n", [6, 11])
-def test_group_commit_unblinded_and_optional_outputs(L, log_n):
-    """No blinding scalars, no coefficient / half-coset / tile-root outputs, padded column stride."""
+@pytest.mark.parametrize("log_n,pad", [(6, 12), (11, 12), (12, 3)])
+def test_group_commit_unblinded_and_optional_outputs(L, log_n, pad):
+    """No blinding scalars, no coefficient / half-coset / tile-root outputs, padded
+    column stride (an odd stride takes the word-by-word permutation)."""
     n, nc = 1 << log_n, 5
     cols = np.stack([O.seeded_m31(0x7300 + c, n) for c in range(nc)])
-    got = run_group(L, cols, log_n, None, stride=n + 12, want=())
+    got = run_group(L, cols, log_n, None, stride=n + pad, want=())
     check(got, O.commit_group_cairo(cols, log_n))
+
+
+@pytest.mark.parametrize("log_n", [9, 12])
+def test_group_commit_half_coset_copy_with_odd_stride_blinded(L, log_n):
+    """Blinded group with an odd input stride: word permutation in, tiled blind + copy out."""
+    n, nc = 1 << log_n, 3
+    cols = np.stack([O.seeded_m31(0x7350 + c, n) for c in range(nc)])
+    blind = [5, 0, P - 2]
+    check(run_group(L, cols, log_n, blind, stride=n + 1), O.commit_group_cairo(cols, log_n, blind))
 
 
 def test_group_commit_three_groups_of_34_columns(L):
@@ -116,15 +126,21 @@ def tail_inputs(log_n, nt, ni, seed):
     return cairo_tail_inputs(log_n, nt, ni, seed)
 
 
-def run_gpu_tail(inp, log_n):
+def run_gpu_tail(inp, log_n, offset=0):
+    """offset > 0 places every input column that many words past an allocation
+    start (word-aligned only), which takes the word-access fallbacks."""
     from vortexstark_b200 import api
     ch = api.Channel()
     ch.mix_digest(inp["root"])
     nt = inp["coeffs"].shape[0]
-    tc = [dev(inp["coeffs"][c]) for c in range(nt)]
-    te = [dev(inp["evals"][c]) for c in range(nt)]
-    ie = [dev(inp["inter"][c]) for c in range(inp["inter"].shape[0])]
-    qh = [dev(inp["q_hc"][k]) for k in range(4)]
+
+    def put(a):
+        t = dev(np.concatenate([np.zeros(offset, np.uint32), a]))
+        return t[offset:] if offset else t
+    tc = [put(inp["coeffs"][c]) for c in range(nt)]
+    te = [put(inp["evals"][c]) for c in range(nt)]
+    ie = [put(inp["inter"][c]) for c in range(inp["inter"].shape[0])]
+    qh = [put(inp["q_hc"][k]) for k in range(4)]
     N = 4 << log_n
     oq = [empty(N) for _ in range(4)]
     qcn = [empty(N) for _ in range(4)]
@@ -139,13 +155,14 @@ def run_gpu_tail(inp, log_n):
     return r, ch
 
 
-@pytest.mark.parametrize("log_n,nt,ni", [(2, 1, 0), (4, 3, 4), (6, 34, 12), (8, 16, 5), (9, 2, 12)])
-def test_cairo_tail_matches_oracle(L, log_n, nt, ni):
+@pytest.mark.parametrize("log_n,nt,ni,offset", [(2, 1, 0, 0), (4, 3, 4, 0), (6, 34, 12, 0), (8, 16, 5, 0),
+                                                (9, 2, 12, 0), (10, 5, 4, 1), (6, 3, 2, 3)])
+def test_cairo_tail_matches_oracle(L, log_n, nt, ni, offset):
     inp = tail_inputs(log_n, nt, ni, 0x7600 + log_n)
     ref_ch = O.Channel()
     ref_ch.mix_digest(inp["root"])
     ref = O.cairo_oods_fri(ref_ch, log_n, inp["coeffs"], inp["zk"], inp["evals"], inp["inter"], inp["q_hc"])
-    got, ch = run_gpu_tail(inp, log_n)
+    got, ch = run_gpu_tail(inp, log_n, offset)
     for k in ("quotient_root", "oods_point", "trace_at_z", "trace_at_z_next", "quotient_at_z", "oods_alpha",
               "oods_root", "last_layer", "last_layer_coeffs", "oods_quotient", "quotient_tiles", "oods_tiles"):
         assert np.array_equal(np.array(got[k], np.uint32).reshape(ref[k].shape), ref[k]), k
@@ -180,12 +197,16 @@ def test_cairo_tail_full_width_is_low_degree(L, log_n):
     cols = api.fill_uniform_m31(torch.empty((34, n), dtype=torch.int32, device=devc), seed=0x7700 + log_n)
     blind = [(0x2468ACE + 7919 * c) % P for c in range(34)]
     coeffs = torch.empty((34, n), dtype=torch.int32, device=devc)
+    evals_hc = torch.empty((34, N), dtype=torch.int32, device=devc)
     evals, ch = [], api.Channel()
     for lo, hi in ((0, 16), (16, 31), (31, 34)):
-        ev, root = api.commit_group_cairo(cols[lo:hi].contiguous(), log_n, blind[lo:hi], coeffs=coeffs[lo:hi])
+        ev, root = api.commit_group_cairo(cols[lo:hi].contiguous(), log_n, blind[lo:hi], coeffs=coeffs[lo:hi],
+                                          eval_hc=evals_hc[lo:hi])
         evals.append(ev)
         ch.mix_digest(host(root))
     evals = torch.cat(evals)
+    pos = _hc_index_map_dev(log_n + 2, devc)
+    assert torch.equal(evals_hc, evals[:, pos])  # the half-coset copy is the inverse permutation
     inter_src = api.fill_uniform_m31(torch.empty((12, n), dtype=torch.int32, device=devc), seed=0x7800 + log_n)
     inter = api.lde_stwo(inter_src, log_n, 2)
     q_src = api.fill_uniform_m31(torch.empty((4, 2 * n), dtype=torch.int32, device=devc), seed=0x7900 + log_n)

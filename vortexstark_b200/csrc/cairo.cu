@@ -48,6 +48,83 @@ __global__ void permute_kernel(const uint32_t* __restrict__ src, uint64_t src_st
   else d[k] = s[j];
 }
 
+// Tiled form of the same permutation for n = 2^L >= 2^11 words. With k = 2m + e
+// (e the parity, m of L-1 bits), the canonic index is cn = e ? ~m : m over L-1
+// bits with e on top, so pos(k) = 2 (brev_{L-1}(m) ^ (e ? mask : 0)) + e: the even
+// words of the half-coset order are bit-reversed into the even canonic words, and
+// the odd words into the odd canonic words in descending order. Split m =
+// (hi | mid | lo) with 5-bit hi and lo. One CTA moves the 32 x 32 (hi, lo) tile
+// of a mid value M and the tile of its complement ~M: the odd words of M's tile
+// land beside the even words of ~M's tile, so each 64-word destination window is
+// written whole. k-side: 32 rows per tile of 64 consecutive words (fixed hi);
+// j-side: 32 windows per tile of 64 consecutive words (fixed lo). Both sides move
+// 8-byte pairs per lane; the shared tile is [tile][parity][hi][lo] with a 33-word
+// pitch, so the bit-reversed side reads it without bank conflicts.
+// TO_CANONIC reads k-rows and writes j-windows; the reverse reads j-windows (and,
+// with zh, blinds them in place: word += r_col * zh, written back) and writes
+// k-rows. The host checks that every column start and stride allows 8-byte access.
+constexpr uint32_t PT_BITS = 5;
+struct Blind16 {
+  uint32_t r[16];
+};
+__device__ __forceinline__ uint32_t brev5(uint32_t x) { return __brev(x) >> 27; }
+
+template <bool TO_CANONIC>
+__global__ void __launch_bounds__(256) permute_tiled_kernel(uint32_t* src, uint64_t src_stride, uint32_t* dst,
+                                                            uint64_t dst_stride, uint32_t L,
+                                                            const uint32_t* __restrict__ zh, Blind16 bl) {
+  __shared__ uint32_t S[2][2][32][33];
+  const uint32_t Lm = L - 1, Md = Lm - 2 * PT_BITS;
+  const uint32_t col = blockIdx.y;
+  uint32_t* s = src + col * src_stride;
+  uint32_t* d = dst + col * dst_stride;
+  const int ntile = Md == 0 ? 1 : 2;
+  const uint32_t M = blockIdx.x, Mb = (~M) & ((1u << Md) - 1);
+  const uint32_t mids[2] = {M, Mb};
+  const uint32_t brmid[2] = {brev(M, Md), brev(Mb, Md)};
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t r = (!TO_CANONIC && zh && col < 16) ? bl.r[col] : 0u;
+  if (TO_CANONIC) {
+    for (uint32_t row = warp; row < ntile * 32u; row += 8) {
+      const uint32_t X = row >> 5, hi = row & 31;
+      const uint64_t m_row = ((uint64_t)hi << (Lm - PT_BITS)) | ((uint64_t)mids[X] << PT_BITS);
+      const uint2 v = *reinterpret_cast<const uint2*>(s + 2 * m_row + 2 * lane);
+      S[X][0][hi][lane] = v.x;
+      S[X][1][hi][lane] = v.y;
+    }
+  } else {
+    for (uint32_t w = warp; w < ntile * 32u; w += 8) {
+      const uint32_t X = w >> 5, lo = w & 31, Xb = ntile == 2 ? 1 - X : 0;
+      const uint64_t base = ((uint64_t)brev5(lo) << (Lm - PT_BITS)) | ((uint64_t)brmid[X] << PT_BITS);
+      uint2* p = reinterpret_cast<uint2*>(s + 2 * base + 2 * lane);
+      uint2 v = *p;
+      if (r) {
+        const uint2 z = *reinterpret_cast<const uint2*>(zh + 2 * base + 2 * lane);
+        v.x = add(v.x, mul(r, z.x));
+        v.y = add(v.y, mul(r, z.y));
+        *p = v;
+      }
+      S[X][0][brev5(lane)][lo] = v.x;
+      S[Xb][1][31 - brev5(lane)][31 - lo] = v.y;
+    }
+  }
+  __syncthreads();
+  if (TO_CANONIC) {
+    for (uint32_t w = warp; w < ntile * 32u; w += 8) {
+      const uint32_t X = w >> 5, lo = w & 31, Xb = ntile == 2 ? 1 - X : 0;
+      const uint64_t base = ((uint64_t)brev5(lo) << (Lm - PT_BITS)) | ((uint64_t)brmid[X] << PT_BITS);
+      *reinterpret_cast<uint2*>(d + 2 * base + 2 * lane) =
+          make_uint2(S[X][0][brev5(lane)][lo], S[Xb][1][31 - brev5(lane)][31 - lo]);
+    }
+  } else {
+    for (uint32_t row = warp; row < ntile * 32u; row += 8) {
+      const uint32_t X = row >> 5, hi = row & 31;
+      const uint64_t m_row = ((uint64_t)hi << (Lm - PT_BITS)) | ((uint64_t)mids[X] << PT_BITS);
+      *reinterpret_cast<uint2*>(d + 2 * m_row + 2 * lane) = make_uint2(S[X][0][hi][lane], S[X][1][hi][lane]);
+    }
+  }
+}
+
 // Z_H (the vanishing polynomial of half_coset(log_n)) at the BRT-canonic points of
 // the evaluation domain: point i = half_odds(log_eval - 1).at(b) for b = brev(i) <
 // N/2, its conjugate at b - N/2 otherwise; Z_H(p) = x(p * R) doubled log_n - 1
@@ -83,7 +160,7 @@ __global__ void axpy_kernel(uint32_t r, const uint32_t* __restrict__ x, uint32_t
 // multiplies by the segment's HI entry and adds it to its total. Each CTA writes
 // one partial sum per point; the host adds the partials (field addition is exact,
 // so the grouping does not change the result).
-constexpr int EV_THREADS = 256, EV_PER = 8, EV_LOG_SEG = 11;  // 2^11 = EV_THREADS * EV_PER
+constexpr int EV_THREADS = 256, EV_PER = 4, EV_LOG_SEG = 10, EV_UNROLL = 2;  // 2^10 = EV_THREADS * EV_PER
 constexpr int EV_MAX_POINTS = 2;
 struct EvMaps {
   qm31 m[EV_MAX_POINTS][30];
@@ -109,11 +186,13 @@ __global__ void basis_table_kernel(EvMaps mp, uint32_t np, uint32_t h, uint32_t 
 __device__ __forceinline__ uint64_t ev_fold(uint64_t a) { return (a & VS_P) + (a >> 31); }
 __device__ __forceinline__ uint32_t ev_reduce(uint64_t a) { return canon((uint32_t)ev_fold(ev_fold(a))); }
 
+// Each CTA takes EV_UNROLL adjacent segments per step so that EV_UNROLL * EV_PER
+// independent loads per thread are in flight; two CTAs fit per SM.
 template <int NP>
-__global__ void __launch_bounds__(EV_THREADS) eval_points_kernel(const uint32_t* const* __restrict__ cols, uint32_t h,
-                                                                 uint32_t lo_n, uint32_t hi_n,
-                                                                 const qm31* __restrict__ tables,
-                                                                 uint32_t* __restrict__ partials) {
+__global__ void __launch_bounds__(EV_THREADS, 2) eval_points_kernel(const uint32_t* const* __restrict__ cols,
+                                                                    uint32_t h, uint32_t lo_n, uint32_t hi_n,
+                                                                    const qm31* __restrict__ tables,
+                                                                    uint32_t* __restrict__ partials) {
   const uint32_t* col = cols[blockIdx.y];
   const uint32_t seg = 1u << h, per = lo_n + hi_n;
   qm31 lo[NP][EV_PER];
@@ -127,29 +206,34 @@ __global__ void __launch_bounds__(EV_THREADS) eval_points_kernel(const uint32_t*
   qm31 tot[NP];
 #pragma unroll
   for (int p = 0; p < NP; p++) tot[p] = qzero();
-  for (uint32_t s = blockIdx.x; s < hi_n; s += gridDim.x) {
-    const uint32_t* base = col + (uint64_t)s * seg;
-    uint32_t x[EV_PER];
+  for (uint32_t s0 = blockIdx.x * EV_UNROLL; s0 < hi_n; s0 += gridDim.x * EV_UNROLL) {
+    uint32_t x[EV_UNROLL][EV_PER];
 #pragma unroll
-    for (int j = 0; j < EV_PER; j++) {
-      const uint32_t i = threadIdx.x + j * EV_THREADS;
-      x[j] = i < seg ? __ldg(base + i) : 0u;
-    }
-#pragma unroll
-    for (int p = 0; p < NP; p++) {
-      uint64_t acc[4] = {0, 0, 0, 0};
+    for (int u = 0; u < EV_UNROLL; u++)
 #pragma unroll
       for (int j = 0; j < EV_PER; j++) {
-#pragma unroll
-        for (int l = 0; l < 4; l++) acc[l] += (uint64_t)x[j] * lo[p][j].v[l];
-        if (j % 3 == 2)
-#pragma unroll
-          for (int l = 0; l < 4; l++) acc[l] = ev_fold(acc[l]);
+        const uint32_t i = threadIdx.x + j * EV_THREADS;
+        x[u][j] = (s0 + u < hi_n && i < seg) ? __ldg(col + (uint64_t)(s0 + u) * seg + i) : 0u;
       }
-      qm31 part;
 #pragma unroll
-      for (int l = 0; l < 4; l++) part.v[l] = ev_reduce(acc[l]);
-      tot[p] = qadd(tot[p], qmul(part, tables[p * per + lo_n + s]));
+    for (int u = 0; u < EV_UNROLL; u++) {
+      if (s0 + u >= hi_n) break;
+#pragma unroll
+      for (int p = 0; p < NP; p++) {
+        uint64_t acc[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < EV_PER; j++) {
+#pragma unroll
+          for (int l = 0; l < 4; l++) acc[l] += (uint64_t)x[u][j] * lo[p][j].v[l];
+          if (j % 3 == 2)
+#pragma unroll
+            for (int l = 0; l < 4; l++) acc[l] = ev_fold(acc[l]);
+        }
+        qm31 part;
+#pragma unroll
+        for (int l = 0; l < 4; l++) part.v[l] = ev_reduce(acc[l]);
+        tot[p] = qadd(tot[p], qmul(part, tables[p * per + lo_n + s0 + u]));
+      }
     }
   }
   __shared__ uint32_t red[EV_THREADS / 32][NP * 4];
@@ -221,6 +305,41 @@ void release_zh_tables() {
   g_zh.clear();
 }
 
+// dst = src permuted to BRT-canonic order (to_canonic) or back to half-coset
+// natural order, n_cols columns of 2^L words. In the reverse direction a non-null
+// zh blinds column c of src in place first (src += r16[c] * zh, r16[c] != 0).
+// Tiled kernel when the sizes and alignment allow 8-byte access, else word
+// kernels (plus the separate blinding pass).
+int launch_permute(bool to_canonic, uint32_t* src, uint64_t src_stride, uint32_t* dst, uint64_t dst_stride,
+                   uint32_t n_cols, uint32_t L, const uint32_t* zh, const uint32_t* r16, cudaStream_t st) {
+  if (n_cols == 0) return VS_OK;
+  if (n_cols > 65535 || (zh && n_cols > 16)) return set_error(VS_ERR_INVALID, "permute: column count");
+  const auto a8 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7) == 0; };
+  const bool tiled = L >= 2 * PT_BITS + 1 && a8(src) && a8(dst) &&
+                     (n_cols == 1 || (src_stride % 2 == 0 && dst_stride % 2 == 0));
+  Blind16 bl{};
+  for (uint32_t c = 0; zh && c < n_cols; c++) bl.r[c] = r16[c];
+  if (tiled) {
+    const uint32_t Md = L - 1 - 2 * PT_BITS;
+    const dim3 grid(Md == 0 ? 1u : 1u << (Md - 1), n_cols);
+    if (to_canonic) permute_tiled_kernel<true><<<grid, 256, 0, st>>>(src, src_stride, dst, dst_stride, L, nullptr, bl);
+    else permute_tiled_kernel<false><<<grid, 256, 0, st>>>(src, src_stride, dst, dst_stride, L, zh, bl);
+    VS_LAUNCHED("permute_tiled_kernel");
+    return VS_OK;
+  }
+  const uint64_t n = 1ull << L;
+  for (uint32_t c = 0; zh && c < n_cols; c++) {
+    if (!bl.r[c]) continue;
+    axpy_kernel<<<blocks_for(n, 256), 256, 0, st>>>(bl.r[c], zh, src + c * src_stride, n);
+    VS_LAUNCHED("axpy_kernel");
+  }
+  const dim3 grid(blocks_for(n, 256), n_cols);
+  if (to_canonic) permute_kernel<true><<<grid, 256, 0, st>>>(src, src_stride, dst, dst_stride, L);
+  else permute_kernel<false><<<grid, 256, 0, st>>>(src, src_stride, dst, dst_stride, L);
+  VS_LAUNCHED("permute_kernel");
+  return VS_OK;
+}
+
 namespace {
 // Stream-ordered allocations released (stream-ordered) when the holder goes out of scope.
 struct Scratch {
@@ -271,7 +390,8 @@ int eval_at_points(const uint32_t* const* h_cols, uint32_t n_cols, uint32_t L, c
   }
   const uint32_t hb = std::min<uint32_t>(L, EV_LOG_SEG);
   const uint32_t lo_n = 1u << hb, hi_n = 1u << (L - hb), per = lo_n + hi_n;
-  const uint32_t gx = std::max<uint32_t>(1, std::min<uint32_t>(hi_n, (uint32_t)sm_count() * 8 / n_cols));
+  const uint32_t gx = std::max<uint32_t>(
+      1, std::min<uint32_t>((hi_n + EV_UNROLL - 1) / EV_UNROLL, (uint32_t)sm_count() * 4 / n_cols));
   Scratch s(st);
   qm31* tables = nullptr;
   uint32_t* partials = nullptr;
@@ -322,10 +442,7 @@ extern "C" int vs_commit_group_cairo(const uint32_t* d_cols_hc, uint64_t col_str
   // 1. half-coset natural -> BRT-canonic (into a stream-ordered scratch)
   uint32_t* cn = nullptr;
   VS_CUDA(cudaMallocAsync((void**)&cn, n_cols * n * 4, st));
-  int rc = VS_OK;
-  permute_kernel<true><<<dim3(blocks_for(n, 256), n_cols), 256, 0, st>>>(d_cols_hc, col_stride, cn, n, log_n);
-  rc = check_cuda(cudaGetLastError(), "permute to canonic");
-  count_launch();
+  int rc = launch_permute(true, const_cast<uint32_t*>(d_cols_hc), col_stride, cn, n, n_cols, log_n, nullptr, nullptr, st);
   // 2. stwo coefficients (the reference keeps them for the OODS evaluation)
   if (rc == VS_OK && d_coeffs) {
     rc = check_cuda(cudaMemcpyAsync(d_coeffs, cn, n_cols * n * 4, cudaMemcpyDeviceToDevice, st), "coeffs copy");
@@ -337,24 +454,22 @@ extern "C" int vs_commit_group_cairo(const uint32_t* d_cols_hc, uint64_t col_str
   // 3. LDE x4 on the canonic coset, BRT output
   if (rc == VS_OK) rc = lde_cached(TW_STWO, cn, n, d_eval_cn, N, n_cols, log_n, 2, st);
   cudaFreeAsync(cn, st);
-  // 4. ZK blinding: column c += r_c * Z_H
-  if (rc == VS_OK && h_blind) {
-    const uint32_t* zh = nullptr;
+  // 4-5. ZK blinding (column c += r_c * Z_H) and the half-coset natural copy
+  // that the reference's constraint kernels read, fused into one pass when both
+  // are asked for
+  const uint32_t* zh = nullptr;
+  bool any_blind = false;
+  for (uint32_t c = 0; h_blind && c < n_cols; c++) any_blind = any_blind || h_blind[c] != 0;
+  if (rc == VS_OK && any_blind) rc = zh_table(log_n, log_eval, st, &zh);
+  if (rc == VS_OK && d_eval_hc) {
+    rc = launch_permute(false, d_eval_cn, N, d_eval_hc, N, n_cols, log_eval, any_blind ? zh : nullptr, h_blind, st);
+  } else if (rc == VS_OK && any_blind) {
     for (uint32_t c = 0; c < n_cols && rc == VS_OK; c++) {
       if (!h_blind[c]) continue;
-      if (!zh) rc = zh_table(log_n, log_eval, st, &zh);
-      if (rc == VS_OK) {
-        axpy_kernel<<<blocks_for(N, 256), 256, 0, st>>>(h_blind[c], zh, d_eval_cn + c * N, N);
-        rc = check_cuda(cudaGetLastError(), "blinding");
-        count_launch();
-      }
+      axpy_kernel<<<blocks_for(N, 256), 256, 0, st>>>(h_blind[c], zh, d_eval_cn + c * N, N);
+      rc = check_cuda(cudaGetLastError(), "blinding");
+      count_launch();
     }
-  }
-  // 5. half-coset natural copy of the evaluations (the reference's constraint kernels read it)
-  if (rc == VS_OK && d_eval_hc) {
-    permute_kernel<false><<<dim3(blocks_for(N, 256), n_cols), 256, 0, st>>>(d_eval_cn, N, d_eval_hc, N, log_eval);
-    rc = check_cuda(cudaGetLastError(), "permute to half-coset");
-    count_launch();
   }
   // 6. commitment: native capped leaf over the group's columns, root + 1024-leaf tile roots
   if (rc == VS_OK) {
@@ -475,8 +590,8 @@ extern "C" int vs_cairo_oods_fri(void* channel, vs_cairo_oods_fri_io* io, vs_str
   for (int k = 0; k < 4; k++) {
     qcn[k] = io->quotient_cn[k];
     if (!qcn[k]) VS_TRY(s.alloc(&qcn[k], N));
-    permute_kernel<true><<<dim3(blocks_for(N, 256), 1), 256, 0, st>>>(io->quotient_hc[k], N, qcn[k], N, log_eval);
-    VS_LAUNCHED("permute_kernel");
+    VS_TRY(launch_permute(true, const_cast<uint32_t*>(io->quotient_hc[k]), N, qcn[k], N, 1, log_eval, nullptr, nullptr,
+                          st));
   }
   uint32_t* qtiles = io->quotient_tile_roots;
   if (!qtiles) VS_TRY(s.alloc(&qtiles, n_tiles * 8));
@@ -582,8 +697,20 @@ extern "C" int vs_cairo_oods_fri(void* channel, vs_cairo_oods_fri_io* io, vs_str
   VS_TRY(s.alloc(&numer, 8 * N));
   uint32_t* const num_z[4] = {numer, numer + N, numer + 2 * N, numer + 3 * N};
   uint32_t* const num_n[4] = {numer + 4 * N, numer + 5 * N, numer + 6 * N, numer + 7 * N};
-  VS_TRY(launch_accumulate_numerators(d_cols, d_iz, d_bz, d_cz, n_all, (uint32_t)N, num_z, vec, st));
-  VS_TRY(launch_accumulate_numerators(d_cols, d_in, d_bn, d_cn, nt + ni, (uint32_t)N, num_n, vec, st));
+  if (vec) {  // one pass over the columns for both samples
+    std::vector<uint32_t> cb(4 * n_all, 0u);
+    std::copy(cn.begin(), cn.begin() + 4 * nt, cb.begin());
+    std::copy(cn.begin() + 4 * nt, cn.end(), cb.begin() + 4 * (nt + 4));
+    uint32_t* d_cb;
+    VS_TRY(s.upload(&d_cb, cb.data(), cb.size()));
+    h::Q sa{{0, 0, 0, 0}}, sb{{0, 0, 0, 0}};
+    for (size_t i = 0; i < bz.size(); i += 4) sa = h::qadd(sa, h::Q{{bz[i], bz[i + 1], bz[i + 2], bz[i + 3]}});
+    for (size_t i = 0; i < bn.size(); i += 4) sb = h::qadd(sb, h::Q{{bn[i], bn[i + 1], bn[i + 2], bn[i + 3]}});
+    VS_TRY(launch_accumulate_numerators2(d_cols, d_cz, d_cb, sa.v, sb.v, n_all, (uint32_t)N, num_z, num_n, st));
+  } else {
+    VS_TRY(launch_accumulate_numerators(d_cols, d_iz, d_bz, d_cz, n_all, (uint32_t)N, num_z, false, st));
+    VS_TRY(launch_accumulate_numerators(d_cols, d_in, d_bn, d_cn, nt + ni, (uint32_t)N, num_n, false, st));
+  }
 
   // BRT-canonic domain points and the combination (prover.rs:2213-2266)
   uint32_t *xs, *ys;

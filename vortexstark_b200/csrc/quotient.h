@@ -13,6 +13,13 @@ namespace vs {
 int launch_accumulate_numerators(const uint32_t* const* d_cols, const uint32_t* d_idx, const uint32_t* d_b,
                                  const uint32_t* d_c, uint32_t n_batch, uint32_t n_rows, uint32_t* const o[4],
                                  bool vec, cudaStream_t st);
+// Two numerators from one pass over the columns: oa = sum_k ca_k cols[k] - bsum_a,
+// ob = sum_k cb_k cols[k] - bsum_b (cb_k = 0 where the second sample does not
+// open column k). ca, cb: device QM31 per column (16-byte aligned); bsums: host.
+// Every column and output must allow 128-bit access and n_rows % 4 == 0.
+int launch_accumulate_numerators2(const uint32_t* const* d_cols, const uint32_t* d_ca, const uint32_t* d_cb,
+                                  const uint32_t bsum_a[4], const uint32_t bsum_b[4], uint32_t n_cols, uint32_t n_rows,
+                                  uint32_t* const oa[4], uint32_t* const ob[4], cudaStream_t st);
 // q[row] = sum_j (numer_j[lift(row)] - A_j y) / D_j(row), tables in device memory.
 int launch_quotients_combine(const uint32_t* spx, const uint32_t* spy, const uint32_t* fla,
                              const uint32_t* const* n0, const uint32_t* const* n1, const uint32_t* const* n2,
