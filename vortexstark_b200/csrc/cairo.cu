@@ -69,17 +69,19 @@ struct Blind16 {
 };
 __device__ __forceinline__ uint32_t brev5(uint32_t x) { return __brev(x) >> 27; }
 
+// The column index varies fastest over the grid, so the CTAs that blind the
+// columns of one tile run together and read that tile of Z_H from L2.
 template <bool TO_CANONIC>
 __global__ void __launch_bounds__(256) permute_tiled_kernel(uint32_t* src, uint64_t src_stride, uint32_t* dst,
-                                                            uint64_t dst_stride, uint32_t L,
+                                                            uint64_t dst_stride, uint32_t L, uint32_t n_cols,
                                                             const uint32_t* __restrict__ zh, Blind16 bl) {
   __shared__ uint32_t S[2][2][32][33];
   const uint32_t Lm = L - 1, Md = Lm - 2 * PT_BITS;
-  const uint32_t col = blockIdx.y;
+  const uint32_t col = blockIdx.x % n_cols;
   uint32_t* s = src + col * src_stride;
   uint32_t* d = dst + col * dst_stride;
   const int ntile = Md == 0 ? 1 : 2;
-  const uint32_t M = blockIdx.x, Mb = (~M) & ((1u << Md) - 1);
+  const uint32_t M = blockIdx.x / n_cols, Mb = (~M) & ((1u << Md) - 1);
   const uint32_t mids[2] = {M, Mb};
   const uint32_t brmid[2] = {brev(M, Md), brev(Mb, Md)};
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -153,14 +155,15 @@ __global__ void axpy_kernel(uint32_t r, const uint32_t* __restrict__ x, uint32_t
 // sum_i c_i prod_{bit b of i} m_b with m_0 = p.y, m_1 = p.x, m_b = pi(m_{b-1}),
 // pi(x) = 2x^2 - 1 (oods.rs:133-161 folds the same products recursively). The
 // basis splits over the low h bits and the rest, basis_i = LO[i mod 2^h] *
-// HI[i >> h]: each thread keeps its EV_PER LO entries per point in registers and
-// walks segments of 2^h coefficients (one coalesced word per thread and entry),
-// takes the dot product of the coefficients with its LO entries per limb in 64
-// bits (folded every three products, as in the numerator kernel), reduces it,
-// multiplies by the segment's HI entry and adds it to its total. Each CTA writes
-// one partial sum per point; the host adds the partials (field addition is exact,
-// so the grouping does not change the result).
-constexpr int EV_THREADS = 256, EV_PER = 4, EV_LOG_SEG = 10, EV_UNROLL = 2;  // 2^10 = EV_THREADS * EV_PER
+// HI[i >> h], so the sum is sum_lo LO[lo] * (sum_s c[s, lo] HI[s]) over segments
+// s of 2^h coefficients. Each thread owns EV_PER positions lo (coalesced words)
+// and accumulates c * HI[s] per limb in 64 bits over the segments it visits:
+// EV_UNROLL segments per step (that many loads per position in flight, and the
+// sums folded once per step, three products per fold as in the numerator kernel).
+// Only at the end are the sums reduced and multiplied by LO. Each CTA writes one
+// partial per point; the host adds the partials (field addition is exact, so the
+// grouping does not change the result).
+constexpr int EV_THREADS = 256, EV_PER = 4, EV_LOG_SEG = 10, EV_UNROLL = 3;  // 2^10 = EV_THREADS * EV_PER
 constexpr int EV_MAX_POINTS = 2;
 struct EvMaps {
   qm31 m[EV_MAX_POINTS][30];
@@ -186,8 +189,6 @@ __global__ void basis_table_kernel(EvMaps mp, uint32_t np, uint32_t h, uint32_t 
 __device__ __forceinline__ uint64_t ev_fold(uint64_t a) { return (a & VS_P) + (a >> 31); }
 __device__ __forceinline__ uint32_t ev_reduce(uint64_t a) { return canon((uint32_t)ev_fold(ev_fold(a))); }
 
-// Each CTA takes EV_UNROLL adjacent segments per step so that EV_UNROLL * EV_PER
-// independent loads per thread are in flight; two CTAs fit per SM.
 template <int NP>
 __global__ void __launch_bounds__(EV_THREADS, 2) eval_points_kernel(const uint32_t* const* __restrict__ cols,
                                                                     uint32_t h, uint32_t lo_n, uint32_t hi_n,
@@ -195,44 +196,52 @@ __global__ void __launch_bounds__(EV_THREADS, 2) eval_points_kernel(const uint32
                                                                     uint32_t* __restrict__ partials) {
   const uint32_t* col = cols[blockIdx.y];
   const uint32_t seg = 1u << h, per = lo_n + hi_n;
-  qm31 lo[NP][EV_PER];
+  uint64_t acc[NP][EV_PER][4];
 #pragma unroll
   for (int p = 0; p < NP; p++)
 #pragma unroll
-    for (int j = 0; j < EV_PER; j++) {
-      const uint32_t i = threadIdx.x + j * EV_THREADS;
-      lo[p][j] = i < seg ? tables[p * per + i] : qzero();
-    }
-  qm31 tot[NP];
+    for (int j = 0; j < EV_PER; j++)
 #pragma unroll
-  for (int p = 0; p < NP; p++) tot[p] = qzero();
+      for (int l = 0; l < 4; l++) acc[p][j][l] = 0;
   for (uint32_t s0 = blockIdx.x * EV_UNROLL; s0 < hi_n; s0 += gridDim.x * EV_UNROLL) {
     uint32_t x[EV_UNROLL][EV_PER];
 #pragma unroll
-    for (int u = 0; u < EV_UNROLL; u++)
+    for (int u = 0; u < EV_UNROLL; u++) {
+      const bool live = s0 + u < hi_n;
 #pragma unroll
       for (int j = 0; j < EV_PER; j++) {
         const uint32_t i = threadIdx.x + j * EV_THREADS;
-        x[u][j] = (s0 + u < hi_n && i < seg) ? __ldg(col + (uint64_t)(s0 + u) * seg + i) : 0u;
+        x[u][j] = (live && i < seg) ? __ldg(col + (uint64_t)(s0 + u) * seg + i) : 0u;
       }
+    }
 #pragma unroll
-    for (int u = 0; u < EV_UNROLL; u++) {
-      if (s0 + u >= hi_n) break;
+    for (int u = 0; u < EV_UNROLL; u++)
 #pragma unroll
       for (int p = 0; p < NP; p++) {
-        uint64_t acc[4] = {0, 0, 0, 0};
+        const qm31 hs = s0 + u < hi_n ? tables[p * per + lo_n + s0 + u] : qzero();  // same for the whole CTA
 #pragma unroll
-        for (int j = 0; j < EV_PER; j++) {
+        for (int j = 0; j < EV_PER; j++)
 #pragma unroll
-          for (int l = 0; l < 4; l++) acc[l] += (uint64_t)x[u][j] * lo[p][j].v[l];
-          if (j % 3 == 2)
+          for (int l = 0; l < 4; l++) acc[p][j][l] += (uint64_t)x[u][j] * hs.v[l];
+      }
 #pragma unroll
-            for (int l = 0; l < 4; l++) acc[l] = ev_fold(acc[l]);
-        }
-        qm31 part;
+    for (int p = 0; p < NP; p++)
 #pragma unroll
-        for (int l = 0; l < 4; l++) part.v[l] = ev_reduce(acc[l]);
-        tot[p] = qadd(tot[p], qmul(part, tables[p * per + lo_n + s0 + u]));
+      for (int j = 0; j < EV_PER; j++)
+#pragma unroll
+        for (int l = 0; l < 4; l++) acc[p][j][l] = ev_fold(acc[p][j][l]);
+  }
+  qm31 tot[NP];
+#pragma unroll
+  for (int p = 0; p < NP; p++) {
+    tot[p] = qzero();
+#pragma unroll
+    for (int j = 0; j < EV_PER; j++) {
+      const uint32_t i = threadIdx.x + j * EV_THREADS;
+      if (i < seg) {
+        const qm31 part{{ev_reduce(acc[p][j][0]), ev_reduce(acc[p][j][1]), ev_reduce(acc[p][j][2]),
+                         ev_reduce(acc[p][j][3])}};
+        tot[p] = qadd(tot[p], qmul(part, tables[p * per + i]));
       }
     }
   }
@@ -321,9 +330,12 @@ int launch_permute(bool to_canonic, uint32_t* src, uint64_t src_stride, uint32_t
   for (uint32_t c = 0; zh && c < n_cols; c++) bl.r[c] = r16[c];
   if (tiled) {
     const uint32_t Md = L - 1 - 2 * PT_BITS;
-    const dim3 grid(Md == 0 ? 1u : 1u << (Md - 1), n_cols);
-    if (to_canonic) permute_tiled_kernel<true><<<grid, 256, 0, st>>>(src, src_stride, dst, dst_stride, L, nullptr, bl);
-    else permute_tiled_kernel<false><<<grid, 256, 0, st>>>(src, src_stride, dst, dst_stride, L, zh, bl);
+    const uint64_t blocks = (Md == 0 ? 1ull : 1ull << (Md - 1)) * n_cols;
+    if (blocks > 0x7FFFFFFFull) return set_error(VS_ERR_INVALID, "permute: grid too large");
+    if (to_canonic)
+      permute_tiled_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(src, src_stride, dst, dst_stride, L, n_cols, nullptr, bl);
+    else
+      permute_tiled_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(src, src_stride, dst, dst_stride, L, n_cols, zh, bl);
     VS_LAUNCHED("permute_tiled_kernel");
     return VS_OK;
   }

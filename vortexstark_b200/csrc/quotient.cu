@@ -142,70 +142,72 @@ __global__ void accumulate_numerators_kernel(const uint32_t* const* __restrict__
 // samples read mostly the same columns): numer_a = sum_k ca_k f_k - sum b_a and
 // numer_b = sum_k cb_k f_k - sum b_b, with cb_k = 0 for a column the second
 // sample does not open. Same accumulation as above (64-bit multiply-adds folded
-// every three columns); 128-bit row access only (the host checks alignment).
+// every three columns, six columns' loads in flight); each thread takes two
+// consecutive rows with 64-bit accesses (the host checks alignment).
 struct Numer2Out {
   uint32_t* o[8];  // a limbs 0..3, then b limbs 0..3
 };
-__global__ void __launch_bounds__(256) accumulate_numerators2_kernel(
+constexpr int AN2_ROWS = 2;
+__global__ void __launch_bounds__(256, 3) accumulate_numerators2_kernel(
     const uint32_t* const* __restrict__ cols, const uint32_t* __restrict__ ca, const uint32_t* __restrict__ cb,
     uint32_t bsum_a0, uint32_t bsum_a1, uint32_t bsum_a2, uint32_t bsum_a3, uint32_t bsum_b0, uint32_t bsum_b1,
     uint32_t bsum_b2, uint32_t bsum_b3, uint32_t n_cols, uint32_t n_rows, Numer2Out out) {
-  const uint32_t t0 = (blockIdx.x * blockDim.x + threadIdx.x) * AN_ROWS;
+  const uint32_t t0 = (blockIdx.x * blockDim.x + threadIdx.x) * AN2_ROWS;
   if (t0 >= n_rows) return;
-  uint64_t acc[2][AN_ROWS][4];
+  uint64_t acc[2][AN2_ROWS][4];
 #pragma unroll
   for (int a = 0; a < 2; a++)
 #pragma unroll
-    for (int r = 0; r < AN_ROWS; r++)
+    for (int r = 0; r < AN2_ROWS; r++)
 #pragma unroll
       for (int l = 0; l < 4; l++) acc[a][r][l] = 0;
-  auto load = [&](uint32_t k, uint32_t (&f)[AN_ROWS]) {
-    const uint4 v = __ldg(reinterpret_cast<const uint4*>(cols[k] + t0));
-    f[0] = v.x; f[1] = v.y; f[2] = v.z; f[3] = v.w;
-  };
-  auto mac = [&](uint32_t k, const uint32_t (&f)[AN_ROWS]) {
+  auto mac = [&](uint32_t k, uint2 f) {
     const uint4 xa = __ldg(reinterpret_cast<const uint4*>(ca) + k), xb = __ldg(reinterpret_cast<const uint4*>(cb) + k);
     const uint32_t la[4] = {xa.x, xa.y, xa.z, xa.w}, lb[4] = {xb.x, xb.y, xb.z, xb.w};
 #pragma unroll
-    for (int r = 0; r < AN_ROWS; r++)
-#pragma unroll
-      for (int l = 0; l < 4; l++) {
-        acc[0][r][l] += (uint64_t)la[l] * f[r];
-        acc[1][r][l] += (uint64_t)lb[l] * f[r];
-      }
+    for (int l = 0; l < 4; l++) {
+      acc[0][0][l] += (uint64_t)la[l] * f.x;
+      acc[0][1][l] += (uint64_t)la[l] * f.y;
+      acc[1][0][l] += (uint64_t)lb[l] * f.x;
+      acc[1][1][l] += (uint64_t)lb[l] * f.y;
+    }
   };
   auto fold_all = [&]() {
 #pragma unroll
     for (int a = 0; a < 2; a++)
 #pragma unroll
-      for (int r = 0; r < AN_ROWS; r++)
+      for (int r = 0; r < AN2_ROWS; r++)
 #pragma unroll
         for (int l = 0; l < 4; l++) acc[a][r][l] = fold31(acc[a][r][l]);
   };
+  auto ld = [&](uint32_t k) { return __ldg(reinterpret_cast<const uint2*>(cols[k] + t0)); };
   uint32_t k = 0;
+  for (; k + 6 <= n_cols; k += 6) {  // six columns in flight, folded every three
+    const uint2 f0 = ld(k), f1 = ld(k + 1), f2 = ld(k + 2), f3 = ld(k + 3), f4 = ld(k + 4), f5 = ld(k + 5);
+    mac(k, f0);
+    mac(k + 1, f1);
+    mac(k + 2, f2);
+    fold_all();
+    mac(k + 3, f3);
+    mac(k + 4, f4);
+    mac(k + 5, f5);
+    fold_all();
+  }
   for (; k + 3 <= n_cols; k += 3) {
-    uint32_t f0[AN_ROWS], f1[AN_ROWS], f2[AN_ROWS];
-    load(k, f0);
-    load(k + 1, f1);
-    load(k + 2, f2);
+    const uint2 f0 = ld(k), f1 = ld(k + 1), f2 = ld(k + 2);
     mac(k, f0);
     mac(k + 1, f1);
     mac(k + 2, f2);
     fold_all();
   }
-  for (; k < n_cols; k++) {
-    uint32_t f0[AN_ROWS];
-    load(k, f0);
-    mac(k, f0);
-  }
+  for (; k < n_cols; k++) mac(k, ld(k));  // at most two more: no fold needed before the reduction
   const uint32_t bs[2][4] = {{bsum_a0, bsum_a1, bsum_a2, bsum_a3}, {bsum_b0, bsum_b1, bsum_b2, bsum_b3}};
 #pragma unroll
   for (int a = 0; a < 2; a++)
 #pragma unroll
     for (int l = 0; l < 4; l++)
-      *reinterpret_cast<uint4*>(out.o[4 * a + l] + t0) =
-          make_uint4(sub(reduce64(acc[a][0][l]), bs[a][l]), sub(reduce64(acc[a][1][l]), bs[a][l]),
-                     sub(reduce64(acc[a][2][l]), bs[a][l]), sub(reduce64(acc[a][3][l]), bs[a][l]));
+      *reinterpret_cast<uint2*>(out.o[4 * a + l] + t0) =
+          make_uint2(sub(reduce64(acc[a][0][l]), bs[a][l]), sub(reduce64(acc[a][1][l]), bs[a][l]));
 }
 
 // q[row] = sum_j (numer_j[lift(row)] - A_j * y) * D_j(row)^-1 with
@@ -321,10 +323,10 @@ int launch_accumulate_numerators2(const uint32_t* const* d_cols, const uint32_t*
                                   const uint32_t bsum_a[4], const uint32_t bsum_b[4], uint32_t n_cols, uint32_t n_rows,
                                   uint32_t* const oa[4], uint32_t* const ob[4], cudaStream_t st) {
   if (!n_rows) return VS_OK;
-  if (n_rows % AN_ROWS) return set_error(VS_ERR_INVALID, "numerators2: rows not a multiple of %d", AN_ROWS);
+  if (n_rows % AN2_ROWS) return set_error(VS_ERR_INVALID, "numerators2: rows not a multiple of %d", AN2_ROWS);
   Numer2Out out;
   for (int l = 0; l < 4; l++) { out.o[l] = oa[l]; out.o[4 + l] = ob[l]; }
-  accumulate_numerators2_kernel<<<blocks_for(n_rows / AN_ROWS, 256), 256, 0, st>>>(
+  accumulate_numerators2_kernel<<<blocks_for(n_rows / AN2_ROWS, 256), 256, 0, st>>>(
       d_cols, d_ca, d_cb, bsum_a[0], bsum_a[1], bsum_a[2], bsum_a[3], bsum_b[0], bsum_b[1], bsum_b[2], bsum_b[3],
       n_cols, n_rows, out);
   VS_LAUNCHED("accumulate_numerators2_kernel");

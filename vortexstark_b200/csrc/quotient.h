@@ -16,7 +16,7 @@ int launch_accumulate_numerators(const uint32_t* const* d_cols, const uint32_t* 
 // Two numerators from one pass over the columns: oa = sum_k ca_k cols[k] - bsum_a,
 // ob = sum_k cb_k cols[k] - bsum_b (cb_k = 0 where the second sample does not
 // open column k). ca, cb: device QM31 per column (16-byte aligned); bsums: host.
-// Every column and output must allow 128-bit access and n_rows % 4 == 0.
+// Every column and output must allow 64-bit access and n_rows must be even.
 int launch_accumulate_numerators2(const uint32_t* const* d_cols, const uint32_t* d_ca, const uint32_t* d_cb,
                                   const uint32_t bsum_a[4], const uint32_t bsum_b[4], uint32_t n_cols, uint32_t n_rows,
                                   uint32_t* const oa[4], uint32_t* const ob[4], cudaStream_t st);
