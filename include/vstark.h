@@ -313,6 +313,20 @@ int vs_commit_group_cairo(const uint32_t* d_cols_hc, uint64_t col_stride, uint32
                           const uint32_t* h_blind, uint32_t* d_coeffs, uint32_t* d_eval_cn, uint32_t* d_eval_hc,
                           uint32_t* d_root, uint32_t* d_tile_roots, vs_stream_t stream);
 
+/* Decommitment of a tree committed with 1024-leaf tile roots
+ * (merkle.rs:603-619,721-800, cairo_air/prover.rs:2520-2560,4087-4130): for each
+ * leaf index, the leaf's column values (h_values, n_indices x n_cols words; may
+ * be NULL) and its sibling path from leaf to root (h_paths, n_indices x
+ * log_n_leaves hashes). The queried tiles are recomputed on the device from the
+ * columns; the levels above come from d_tile_roots (max(1, 2^log_n_leaves / 1024)
+ * hashes; the root alone for smaller trees). Leaves: VS_LEAF_CAPPED (1..16
+ * columns, the native leaf) or VS_LEAF_SOA4 (4 columns, one QM31 per leaf).
+ * h_cols: host array of device pointers. Synchronises the stream. */
+enum { VS_LEAF_CAPPED = 0, VS_LEAF_SOA4 = 1 };
+int vs_tile_tree_paths(uint32_t leaf_kind, const uint32_t* const* h_cols, uint32_t n_cols, uint32_t log_n_leaves,
+                       const uint32_t* d_tile_roots, const uint64_t* h_indices, uint32_t n_indices,
+                       uint32_t* h_values, uint32_t* h_paths, vs_stream_t stream);
+
 /* Circle polynomials in the stwo coefficient basis evaluated at QM31 points
  * (oods.rs:133-161, eval_at_oods_from_coeffs, which the reference runs on the
  * host per column). h_cols: host array of n_cols device pointers, 2^log_len

@@ -442,3 +442,23 @@ extern "C" void oracle_cairo_oods_fri(ChState* s, uint32_t log_n, const uint32_t
   for (size_t i = 0; i < r.fri_alphas.size(); i++) put(fri_alphas + 4 * i, r.fri_alphas[i]);
   for (int i = 0; i < 8; i++) { put(last32 + 4 * i, r.last_layer[i]); put(coeffs32 + 4 * i, r.last_layer_coeffs[i]); }
 }
+
+// Full-tree auth paths (merkle.rs:846-861) of a capped-leaf (kind 0, <= 16 used
+// columns) or SoA4 (kind 1) tree over flat columns (n_cols x 2^log_n).
+extern "C" void oracle_tree_paths(uint32_t kind, const uint32_t* cols, uint32_t n_cols, uint32_t log_n,
+                                  const uint64_t* idx, uint32_t n_idx, uint32_t* out_paths, int threads) {
+  const uint64_t n = 1ull << log_n;
+  std::vector<Hash> leaves(n);
+  for (uint64_t i = 0; i < n; i++) {
+    uint32_t row[16] = {0};
+    const uint32_t used = std::min<uint32_t>(n_cols, 16);
+    for (uint32_t c = 0; c < used; c++) row[c] = cols[c * n + i];
+    leaves[i] = kind == 1 ? blake2s_words(row, 4) : leaf_hash_capped(row, n_cols);
+  }
+  (void)threads;
+  auto layers = merkle_layers(std::move(leaves));
+  for (uint32_t q = 0; q < n_idx; q++) {
+    auto p = auth_path(layers, idx[q]);
+    for (size_t k = 0; k < p.size(); k++) put_hash(out_paths + ((uint64_t)q * log_n + k) * 8, p[k]);
+  }
+}

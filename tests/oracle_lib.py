@@ -170,6 +170,17 @@ def commit_group_cairo(cols_hc: np.ndarray, log_n: int, blind=None, threads: int
     return {"coeffs": coeffs, "eval_cn": ev_cn, "eval_hc": ev_hc, "root": root, "tile_roots": tiles}
 
 
+def tree_paths(kind: int, cols: np.ndarray, idx) -> np.ndarray:
+    """Auth paths (n_idx, log_n, 8) of a capped-leaf (kind 0) or SoA4 (kind 1) tree."""
+    cols = np.ascontiguousarray(cols, np.uint32)
+    nc, n = cols.shape
+    log_n = n.bit_length() - 1
+    ix = np.ascontiguousarray(idx, np.uint64)
+    out = np.zeros((len(ix), max(log_n, 1), 8), np.uint32)
+    lib().oracle_tree_paths(kind, ptr(cols), nc, log_n, ptr(ix), len(ix), ptr(out), 1)
+    return out[:, :log_n]
+
+
 def bit_reverse(d: np.ndarray, log_n: int) -> np.ndarray:
     d = np.ascontiguousarray(d, np.uint32).copy()
     lib().oracle_bit_reverse(ptr(d), log_n)

@@ -221,3 +221,74 @@ def test_cairo_tail_full_width_is_low_degree(L, log_n):
     for k in range(4):
         assert torch.equal(out_cn[k], q_cn[k])
     assert len(r["fri_roots"]) == log_n - 2
+
+
+# ------------------------------------------------------------------ decommitment of tile-rooted trees
+def _gpu_paths(L, kind, cols_dev, log_n, tiles_dev, idx):
+    nc = len(cols_dev)
+    hc = (C.c_uint64 * nc)(*[ptr(t) for t in cols_dev])
+    ix = (C.c_uint64 * len(idx))(*[int(i) for i in idx])
+    vals = (C.c_uint32 * (len(idx) * nc))()
+    paths = (C.c_uint32 * max(1, len(idx) * log_n * 8))()
+    rc = L.vs_tile_tree_paths(kind, hc, nc, log_n, ptr(tiles_dev), ix, len(idx), vals, paths, None)
+    assert rc == 0, L.vs_last_error()
+    return (np.array(vals, np.uint32).reshape(len(idx), nc),
+            np.array(paths, np.uint32)[: len(idx) * log_n * 8].reshape(len(idx), log_n, 8))
+
+
+def _canonic_next(qi, log_eval):
+    """prover.rs:170-179: the BRT-canonic index one trace step (4 rows) on."""
+    n = 1 << log_eval
+    cn = int(format(qi, f"0{log_eval}b")[::-1], 2)
+    k = 2 * cn if cn < n // 2 else 2 * (n - 1 - cn) + 1
+    kn = (k + 4) % n
+    cnn = kn // 2 if kn % 2 == 0 else n - 1 - kn // 2
+    return int(format(cnn, f"0{log_eval}b")[::-1], 2)
+
+
+@pytest.mark.parametrize("log_n,nc", [(4, 3), (8, 16), (9, 15), (11, 3)])
+def test_trace_group_decommitment_matches_oracle(L, log_n, nc):
+    """Trace-group queries at q and at the next trace row (prover.rs:2510-2560)."""
+    n, N = 1 << log_n, 4 << log_n
+    cols = np.stack([O.seeded_m31(0x7B00 + c, n) for c in range(nc)])
+    blind = [(77 + 13 * c) % P for c in range(nc)]
+    d_cols = dev(cols.reshape(-1))
+    ev = empty(nc * N)
+    root = empty(8)
+    tiles = empty(max(1, N // 1024) * 8)
+    assert L.vs_commit_group_cairo(ptr(d_cols), n, nc, log_n, u32_host(blind), None, ptr(ev), None, ptr(root),
+                                   ptr(tiles), None) == 0, L.vs_last_error()
+    ref = O.commit_group_cairo(cols, log_n, blind)
+    rng = np.random.default_rng(log_n)
+    q = [0, N - 1] + [int(x) for x in rng.integers(0, N, 14)] + [3, 3]
+    idx = q + [_canonic_next(i, log_n + 2) for i in q]
+    cols_dev = [ev[c * N:(c + 1) * N] for c in range(nc)]
+    vals, paths = _gpu_paths(L, 0, cols_dev, log_n + 2, tiles, idx)
+    assert np.array_equal(vals, ref["eval_cn"][:, idx].T)
+    assert np.array_equal(paths, O.tree_paths(0, ref["eval_cn"], idx))
+
+
+@pytest.mark.parametrize("log_n", [4, 9])
+def test_quotient_decommitment_matches_oracle(L, log_n):
+    """SoA4 trees of the tail (AIR quotient and DEEP quotient): queries and their fold siblings."""
+    inp = tail_inputs(log_n, 3, 4, 0x7C00 + log_n)
+    got, _ = run_gpu_tail(inp, log_n)
+    N = 4 << log_n
+    rng = np.random.default_rng(7)
+    q = [int(x) for x in rng.integers(0, N, 20)]
+    idx = q + [i ^ 1 for i in q]
+    for key, tkey in (("quotient_cn", "quotient_tiles"), ("oods_quotient", "oods_tiles")):
+        cols = got[key]
+        vals, paths = _gpu_paths(L, 1, [dev(cols[k]) for k in range(4)], log_n + 2, dev(got[tkey].reshape(-1)), idx)
+        assert np.array_equal(vals, cols[:, idx].T), key
+        assert np.array_equal(paths, O.tree_paths(1, cols, idx)), key
+
+
+def test_tile_tree_paths_rejects_bad_arguments(L):
+    t = empty(64)
+    hc = (C.c_uint64 * 4)(*[ptr(t)] * 4)
+    ix = (C.c_uint64 * 1)(64)
+    out = (C.c_uint32 * 64)()
+    assert L.vs_tile_tree_paths(1, hc, 3, 6, ptr(t), ix, 1, out, out, None) != 0   # SoA4 needs 4 columns
+    assert L.vs_tile_tree_paths(0, hc, 4, 6, ptr(t), ix, 1, out, out, None) != 0   # index out of range
+    assert L.vs_tile_tree_paths(7, hc, 4, 6, ptr(t), ix, 0, out, out, None) != 0   # unknown leaf

@@ -189,3 +189,24 @@ def test_cairo_tail_advances_channel_deterministically():
     assert c1.state_bytes() == c2.state_bytes()
     assert np.array_equal(r1["oods_root"], r2["oods_root"])
     assert c1.state_bytes() != O.Channel().state_bytes()
+
+
+# ---------------------------------------------------------------- decommitment paths (merkle.rs:846-861)
+def _climb(leaf_hash, idx, path):
+    h = leaf_hash
+    for k, sib in enumerate(path):
+        pair = np.concatenate([h, sib]) if ((idx >> k) & 1) == 0 else np.concatenate([sib, h])
+        h = O.blake2s_words(pair)
+    return h
+
+
+@pytest.mark.parametrize("kind,nc,log_n", [(0, 5, 6), (0, 16, 9), (1, 4, 7)])
+def test_oracle_tree_paths_reach_the_root(kind, nc, log_n):
+    n = 1 << log_n
+    cols = np.stack([O.seeded_m31(0x7A00 + c, n) for c in range(nc)])
+    idx = [0, n - 1, 5, 5, n // 2 + 1]
+    paths = O.tree_paths(kind, cols, idx)
+    root = O.merkle_root_capped(cols) if kind == 0 else O.merkle_root_soa4(cols)
+    for q, i in enumerate(idx):
+        leaf = O.blake2s_words(cols[:min(nc, 16), i] if kind == 0 else cols[:4, i])
+        assert np.array_equal(_climb(leaf, i, paths[q]), root)

@@ -452,3 +452,82 @@ extern "C" int vs_prove_fib(uint32_t a, uint32_t b, uint32_t log_n, uint8_t* h_o
   std::copy(bytes.begin(), bytes.end(), h_out);
   return VS_OK;
 }
+
+// ------------------------------------------------------------------ decommitment of tile-rooted trees
+namespace vs {
+// out[q * n_cols + c] = cols[c][idx[q]]
+__global__ void gather_cols_kernel(const uint32_t* const* __restrict__ cols, uint32_t n_cols,
+                                   const uint64_t* __restrict__ idx, uint32_t nq, uint32_t* __restrict__ out) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nq * n_cols) return;
+  const uint32_t q = t / n_cols, c = t % n_cols;
+  out[t] = cols[c][idx[q]];
+}
+
+// Auth paths of a tree whose 1024-leaf tile roots are resident: the levels above
+// the tiles are rebuilt from the tile roots, the queried tiles from their leaves.
+template <class Leaf>
+static int tile_tree_paths(const Leaf& leaf, uint32_t log_n, const uint32_t* d_tile_roots,
+                           const std::vector<uint64_t>& idx, std::vector<std::vector<h::Hash>>& paths, DevMem& mem,
+                           cudaStream_t st) {
+  DevTree t;
+  t.n = 1ull << log_n;
+  t.TL = std::min<uint32_t>(MK_MAX_TL, log_n);
+  uint64_t cnt = t.n >> t.TL;
+  t.layers.push_back(const_cast<uint32_t*>(d_tile_roots));
+  while (cnt > 1) {
+    uint32_t* par = nullptr;
+    VS_TRY(mem.alloc(&par, (cnt / 2) * 8));
+    VS_TRY(launch_hash_nodes(t.layers.back(), par, cnt / 2, st));
+    t.layers.push_back(par);
+    cnt /= 2;
+  }
+  return tree_paths(leaf, t, idx, paths, mem, st);
+}
+}  // namespace vs
+
+extern "C" int vs_tile_tree_paths(uint32_t leaf_kind, const uint32_t* const* h_cols, uint32_t n_cols,
+                                  uint32_t log_n_leaves, const uint32_t* d_tile_roots, const uint64_t* h_indices,
+                                  uint32_t n_indices, uint32_t* h_values, uint32_t* h_paths, vs_stream_t stream) {
+  clear_error();
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!h_cols || !d_tile_roots || (n_indices && (!h_indices || !h_paths)))
+    return set_error(VS_ERR_INVALID, "vs_tile_tree_paths: null argument");
+  if (leaf_kind == VS_LEAF_SOA4 ? n_cols != 4 : (leaf_kind != VS_LEAF_CAPPED || n_cols == 0 || n_cols > 16))
+    return set_error(VS_ERR_INVALID, "vs_tile_tree_paths: leaf kind %u with %u columns", leaf_kind, n_cols);
+  if (log_n_leaves > 30) return set_error(VS_ERR_INVALID, "vs_tile_tree_paths: log_n_leaves %u", log_n_leaves);
+  for (uint32_t c = 0; c < n_cols; c++)
+    if (!h_cols[c]) return set_error(VS_ERR_INVALID, "vs_tile_tree_paths: null column %u", c);
+  const uint64_t n = 1ull << log_n_leaves;
+  std::vector<uint64_t> idx(h_indices, h_indices + n_indices);
+  for (uint64_t i : idx)
+    if (i >= n) return set_error(VS_ERR_INVALID, "vs_tile_tree_paths: index %llu >= %llu", (unsigned long long)i,
+                                 (unsigned long long)n);
+  if (!n_indices) return VS_OK;
+  DevMem mem(st);
+  const uint32_t** d_cols = nullptr;
+  VS_TRY(mem.alloc(&d_cols, n_cols));
+  VS_CUDA(cudaMemcpyAsync(d_cols, h_cols, n_cols * sizeof(void*), cudaMemcpyHostToDevice, st));
+  std::vector<std::vector<h::Hash>> paths;
+  if (leaf_kind == VS_LEAF_SOA4)
+    VS_TRY(tile_tree_paths(LeafSoa4{h_cols[0], h_cols[1], h_cols[2], h_cols[3]}, log_n_leaves, d_tile_roots, idx,
+                           paths, mem, st));
+  else
+    VS_TRY(tile_tree_paths(LeafCapped{d_cols, nullptr, 0, n_cols}, log_n_leaves, d_tile_roots, idx, paths, mem, st));
+  for (uint32_t q = 0; q < n_indices; q++)
+    for (uint32_t k = 0; k < log_n_leaves; k++)
+      std::copy_n(paths[q][k].data(), 8, h_paths + ((uint64_t)q * log_n_leaves + k) * 8);
+  if (h_values) {
+    uint64_t* d_idx;
+    uint32_t* d_out;
+    VS_TRY(mem.alloc(&d_idx, n_indices));
+    VS_TRY(mem.alloc(&d_out, (uint64_t)n_indices * n_cols));
+    VS_CUDA(cudaMemcpyAsync(d_idx, idx.data(), n_indices * 8, cudaMemcpyHostToDevice, st));
+    gather_cols_kernel<<<blocks_for((uint64_t)n_indices * n_cols, 128), 128, 0, st>>>(d_cols, n_cols, d_idx, n_indices,
+                                                                                   d_out);
+    VS_LAUNCHED("gather_cols_kernel");
+    VS_CUDA(cudaMemcpyAsync(h_values, d_out, (uint64_t)n_indices * n_cols * 4, cudaMemcpyDeviceToHost, st));
+    VS_CUDA(cudaStreamSynchronize(st));
+  }
+  return VS_OK;
+}
