@@ -327,6 +327,26 @@ int vs_tile_tree_paths(uint32_t leaf_kind, const uint32_t* const* h_cols, uint32
                        const uint32_t* d_tile_roots, const uint64_t* h_indices, uint32_t n_indices,
                        uint32_t* h_values, uint32_t* h_paths, vs_stream_t stream);
 
+/* stwo wire-format helpers (src/stwo_export.rs:160-330, 700-790), host only.
+ * Positions may come in any order and repeat (the first occurrence counts).
+ * hash witness: from per-query auth paths (h_paths, n x height hashes, leaf level
+ * first) the sibling hashes a verifier cannot compute, level by level in
+ * ascending position order; the fold-pair form opens both members of each
+ * queried pair (FRI layers). fri witness: the partner values (h_sibling_values, 4
+ * words per query, the value at position ^ 1) of queried positions whose partner
+ * is not queried. root from witness: rebuilds the root from the queried rows
+ * (n x n_cols words, leaf = Blake2s of the row's words) and a hash witness,
+ * failing when the witness is short or not used up. out_len counts hashes or
+ * QM31 values written (at most cap). */
+int vs_stwo_hash_witness(const uint64_t* h_positions, uint32_t n, const uint32_t* h_paths, uint32_t height,
+                         uint32_t* h_out, uint32_t cap_hashes, uint32_t* out_len);
+int vs_stwo_fold_pair_hash_witness(const uint64_t* h_positions, uint32_t n, const uint32_t* h_paths, uint32_t height,
+                                   uint32_t* h_out, uint32_t cap_hashes, uint32_t* out_len);
+int vs_stwo_fri_witness(const uint64_t* h_positions, uint32_t n, const uint32_t* h_sibling_values, uint32_t* h_out,
+                        uint32_t cap, uint32_t* out_len);
+int vs_stwo_root_from_witness(uint32_t log_height, const uint64_t* h_positions, uint32_t n, const uint32_t* h_rows,
+                              uint32_t n_cols, const uint32_t* h_witness, uint32_t n_witness, uint32_t* h_root);
+
 /* Circle polynomials in the stwo coefficient basis evaluated at QM31 points
  * (oods.rs:133-161, eval_at_oods_from_coeffs, which the reference runs on the
  * host per column). h_cols: host array of n_cols device pointers, 2^log_len

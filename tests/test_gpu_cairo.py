@@ -207,6 +207,25 @@ def test_cairo_tail_full_width_is_low_degree(L, log_n):
     evals = torch.cat(evals)
     pos = _hc_index_map_dev(log_n + 2, devc)
     assert torch.equal(evals_hc, evals[:, pos])  # the half-coset copy is the inverse permutation
+    # decommit the first group at 80 queries and their next rows, convert the paths
+    # to stwo's hash witness and rebuild the group's root from it
+    rng = np.random.default_rng(log_n)
+    qs = [int(x) for x in rng.integers(0, N, 80)]
+    idx = sorted(set(qs + [_canonic_next(q, log_n + 2) for q in qs]))
+    tiles0 = empty(max(1, N // 1024) * 8)
+    ev0, root0 = api.commit_group_cairo(cols[0:16].contiguous(), log_n, blind[0:16], tile_roots=tiles0)
+    vals, paths = _gpu_paths(L, 0, list(ev0), log_n + 2, tiles0, idx)
+    flat = paths.reshape(-1)
+    wit = (C.c_uint32 * flat.size)()
+    m = C.c_uint32()
+    assert L.vs_stwo_hash_witness((C.c_uint64 * len(idx))(*idx), len(idx), (C.c_uint32 * flat.size)(*flat.tolist()),
+                                  log_n + 2, wit, len(idx) * (log_n + 2), C.byref(m)) == 0
+    rebuilt = (C.c_uint32 * 8)()
+    assert L.vs_stwo_root_from_witness(log_n + 2, (C.c_uint64 * len(idx))(*idx), len(idx),
+                                       (C.c_uint32 * vals.size)(*vals.reshape(-1).tolist()), 16, wit, m.value,
+                                       rebuilt) == 0, L.vs_last_error()
+    assert np.array_equal(np.array(rebuilt, np.uint32), host(root0))
+    assert m.value < len(idx) * (log_n + 2)
     inter_src = api.fill_uniform_m31(torch.empty((12, n), dtype=torch.int32, device=devc), seed=0x7800 + log_n)
     inter = api.lde_stwo(inter_src, log_n, 2)
     q_src = api.fill_uniform_m31(torch.empty((4, 2 * n), dtype=torch.int32, device=devc), seed=0x7900 + log_n)
