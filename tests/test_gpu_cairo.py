@@ -102,14 +102,17 @@ def test_group_commit_rejects_bad_arguments(L):
 
 
 # ------------------------------------------------------------------ evaluation at OODS points
-@pytest.mark.parametrize("log_len,n_cols,n_points", [(2, 1, 1), (5, 3, 2), (11, 2, 2), (12, 5, 1), (16, 3, 2)])
-def test_eval_at_oods_points_matches_oracle(L, log_len, n_cols, n_points):
+@pytest.mark.parametrize("log_len,n_cols,n_points,offset", [(2, 1, 1, 0), (5, 3, 2, 0), (11, 2, 2, 0), (12, 5, 1, 0),
+                                                           (16, 3, 2, 0), (14, 2, 2, 1), (13, 1, 1, 2)])
+def test_eval_at_oods_points_matches_oracle(L, log_len, n_cols, n_points, offset):
+    """Aligned columns of 2^12 words and more take the cp.async ring kernel; an
+    offset of 1 or 2 words takes the register kernel."""
     n = 1 << log_len
     cols = [O.seeded_m31(0x7500 + 7 * log_len + c, n) for c in range(n_cols)]
     ch = O.Channel()
     ch.mix_u64(log_len)
     pts = [ch.oods_point() for _ in range(n_points)]
-    d = [dev(c) for c in cols]
+    d = [dev(np.concatenate([np.zeros(offset, np.uint32), c]))[offset:] for c in cols]
     hc = (C.c_uint64 * n_cols)(*[ptr(t) for t in d])
     hp = u32_host(np.concatenate(pts))
     out = (C.c_uint32 * (4 * n_cols * n_points))()

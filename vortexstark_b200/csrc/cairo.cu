@@ -86,43 +86,71 @@ __global__ void __launch_bounds__(256) permute_tiled_kernel(uint32_t* src, uint6
   const uint32_t brmid[2] = {brev(M, Md), brev(Mb, Md)};
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t r = (!TO_CANONIC && zh && col < 16) ? bl.r[col] : 0u;
+  const uint32_t rows = ntile * 32u;
+  // every warp moves rows / 8 rows (or windows): all of its loads are issued
+  // before any is consumed
+  constexpr int PER_WARP = 8;
   if (TO_CANONIC) {
-    for (uint32_t row = warp; row < ntile * 32u; row += 8) {
-      const uint32_t X = row >> 5, hi = row & 31;
-      const uint64_t m_row = ((uint64_t)hi << (Lm - PT_BITS)) | ((uint64_t)mids[X] << PT_BITS);
-      const uint2 v = *reinterpret_cast<const uint2*>(s + 2 * m_row + 2 * lane);
-      S[X][0][hi][lane] = v.x;
-      S[X][1][hi][lane] = v.y;
+    uint2 v[PER_WARP];
+#pragma unroll
+    for (int i = 0; i < PER_WARP; i++) {
+      const uint32_t row = warp + 8 * i, X = row >> 5, hi = row & 31;
+      const uint64_t m_row = ((uint64_t)hi << (Lm - PT_BITS)) | ((uint64_t)mids[X & 1] << PT_BITS);
+      if (row < rows) v[i] = *reinterpret_cast<const uint2*>(s + 2 * m_row + 2 * lane);
+    }
+#pragma unroll
+    for (int i = 0; i < PER_WARP; i++) {
+      const uint32_t row = warp + 8 * i, X = row >> 5, hi = row & 31;
+      if (row < rows) {
+        S[X][0][hi][lane] = v[i].x;
+        S[X][1][hi][lane] = v[i].y;
+      }
     }
   } else {
-    for (uint32_t w = warp; w < ntile * 32u; w += 8) {
-      const uint32_t X = w >> 5, lo = w & 31, Xb = ntile == 2 ? 1 - X : 0;
-      const uint64_t base = ((uint64_t)brev5(lo) << (Lm - PT_BITS)) | ((uint64_t)brmid[X] << PT_BITS);
-      uint2* p = reinterpret_cast<uint2*>(s + 2 * base + 2 * lane);
-      uint2 v = *p;
-      if (r) {
-        const uint2 z = *reinterpret_cast<const uint2*>(zh + 2 * base + 2 * lane);
-        v.x = add(v.x, mul(r, z.x));
-        v.y = add(v.y, mul(r, z.y));
-        *p = v;
+    uint2 v[PER_WARP], z[PER_WARP];
+#pragma unroll
+    for (int i = 0; i < PER_WARP; i++) {
+      const uint32_t w = warp + 8 * i, X = w >> 5, lo = w & 31;
+      const uint64_t base = ((uint64_t)brev5(lo) << (Lm - PT_BITS)) | ((uint64_t)brmid[X & 1] << PT_BITS);
+      if (w < rows) {
+        v[i] = *reinterpret_cast<const uint2*>(s + 2 * base + 2 * lane);
+        if (r) z[i] = *reinterpret_cast<const uint2*>(zh + 2 * base + 2 * lane);
       }
-      S[X][0][brev5(lane)][lo] = v.x;
-      S[Xb][1][31 - brev5(lane)][31 - lo] = v.y;
+    }
+#pragma unroll
+    for (int i = 0; i < PER_WARP; i++) {
+      const uint32_t w = warp + 8 * i, X = w >> 5, lo = w & 31, Xb = ntile == 2 ? 1 - X : 0;
+      if (w < rows) {
+        if (r) {
+          const uint64_t base = ((uint64_t)brev5(lo) << (Lm - PT_BITS)) | ((uint64_t)brmid[X & 1] << PT_BITS);
+          v[i].x = add(v[i].x, mul(r, z[i].x));
+          v[i].y = add(v[i].y, mul(r, z[i].y));
+          *reinterpret_cast<uint2*>(s + 2 * base + 2 * lane) = v[i];
+        }
+        S[X][0][brev5(lane)][lo] = v[i].x;
+        S[Xb][1][31 - brev5(lane)][31 - lo] = v[i].y;
+      }
     }
   }
   __syncthreads();
   if (TO_CANONIC) {
-    for (uint32_t w = warp; w < ntile * 32u; w += 8) {
-      const uint32_t X = w >> 5, lo = w & 31, Xb = ntile == 2 ? 1 - X : 0;
-      const uint64_t base = ((uint64_t)brev5(lo) << (Lm - PT_BITS)) | ((uint64_t)brmid[X] << PT_BITS);
-      *reinterpret_cast<uint2*>(d + 2 * base + 2 * lane) =
-          make_uint2(S[X][0][brev5(lane)][lo], S[Xb][1][31 - brev5(lane)][31 - lo]);
+#pragma unroll
+    for (int i = 0; i < PER_WARP; i++) {
+      const uint32_t w = warp + 8 * i, X = w >> 5, lo = w & 31, Xb = ntile == 2 ? 1 - X : 0;
+      if (w < rows) {
+        const uint64_t base = ((uint64_t)brev5(lo) << (Lm - PT_BITS)) | ((uint64_t)brmid[X & 1] << PT_BITS);
+        *reinterpret_cast<uint2*>(d + 2 * base + 2 * lane) =
+            make_uint2(S[X][0][brev5(lane)][lo], S[Xb][1][31 - brev5(lane)][31 - lo]);
+      }
     }
   } else {
-    for (uint32_t row = warp; row < ntile * 32u; row += 8) {
-      const uint32_t X = row >> 5, hi = row & 31;
-      const uint64_t m_row = ((uint64_t)hi << (Lm - PT_BITS)) | ((uint64_t)mids[X] << PT_BITS);
-      *reinterpret_cast<uint2*>(d + 2 * m_row + 2 * lane) = make_uint2(S[X][0][hi][lane], S[X][1][hi][lane]);
+#pragma unroll
+    for (int i = 0; i < PER_WARP; i++) {
+      const uint32_t row = warp + 8 * i, X = row >> 5, hi = row & 31;
+      if (row < rows) {
+        const uint64_t m_row = ((uint64_t)hi << (Lm - PT_BITS)) | ((uint64_t)mids[X & 1] << PT_BITS);
+        *reinterpret_cast<uint2*>(d + 2 * m_row + 2 * lane) = make_uint2(S[X][0][hi][lane], S[X][1][hi][lane]);
+      }
     }
   }
 }
@@ -243,6 +271,103 @@ __global__ void __launch_bounds__(EV_THREADS, 2) eval_points_kernel(const uint32
                          ev_reduce(acc[p][j][3])}};
         tot[p] = qadd(tot[p], qmul(part, tables[p * per + i]));
       }
+    }
+  }
+  __shared__ uint32_t red[EV_THREADS / 32][NP * 4];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int p = 0; p < NP; p++)
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      uint32_t v = tot[p].v[l];
+#pragma unroll
+      for (int off = 16; off; off >>= 1) v = add(v, __shfl_down_sync(0xFFFFFFFFu, v, off));
+      if (lane == 0) red[warp][p * 4 + l] = v;
+    }
+  __syncthreads();
+  if (threadIdx.x < NP * 4) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int w = 0; w < EV_THREADS / 32; w++) v = add(v, red[w][threadIdx.x]);
+    partials[((uint64_t)blockIdx.y * gridDim.x + blockIdx.x) * (NP * 4) + threadIdx.x] = v;
+  }
+}
+
+// The same sums with the coefficients streamed through a per-thread cp.async
+// ring: thread t owns the four consecutive positions 4t..4t+3 of every segment
+// (one 16-byte copy per segment), EVR_STAGES - 1 segments ahead of the one it
+// multiplies; it reads back only the slots it filled, so no barrier is needed.
+// Needs 16-byte aligned columns and segments of 1024 words (the host checks).
+constexpr int EVR_STAGES = 8;
+__device__ __forceinline__ void cp_async16_cg(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_grp() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_grp() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int NP>
+__global__ void __launch_bounds__(EV_THREADS, 2) eval_points_ring_kernel(const uint32_t* const* __restrict__ cols,
+                                                                         uint32_t lo_n, uint32_t hi_n,
+                                                                         const qm31* __restrict__ tables,
+                                                                         uint32_t* __restrict__ partials) {
+  __shared__ uint4 ring[EVR_STAGES][EV_THREADS];
+  const uint32_t* col = cols[blockIdx.y] + 4 * threadIdx.x;
+  const uint32_t per = lo_n + hi_n;
+  const uint32_t slot0 = (uint32_t)__cvta_generic_to_shared(&ring[0][threadIdx.x]);
+  constexpr uint32_t SLOT_STRIDE = EV_THREADS * sizeof(uint4);
+  uint64_t acc[NP][4][4];
+#pragma unroll
+  for (int p = 0; p < NP; p++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int l = 0; l < 4; l++) acc[p][j][l] = 0;
+  // this CTA's segments: s_i = blockIdx.x + i * gridDim.x
+  const uint32_t n_mine = blockIdx.x < hi_n ? (hi_n - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+#pragma unroll
+  for (uint32_t i = 0; i < EVR_STAGES - 1; i++) {
+    if (i < n_mine) cp_async16_cg(slot0 + i * SLOT_STRIDE, col + (uint64_t)(blockIdx.x + i * gridDim.x) * lo_n);
+    cp_async_commit_grp();
+  }
+  for (uint32_t i = 0; i < n_mine; i++) {
+    const uint32_t ni = i + EVR_STAGES - 1;
+    if (ni < n_mine)
+      cp_async16_cg(slot0 + (ni % EVR_STAGES) * SLOT_STRIDE, col + (uint64_t)(blockIdx.x + ni * gridDim.x) * lo_n);
+    cp_async_commit_grp();
+    cp_async_wait_grp<EVR_STAGES - 1>();
+    const uint4 v = ring[i % EVR_STAGES][threadIdx.x];
+    const uint32_t x[4] = {v.x, v.y, v.z, v.w};
+    const uint32_t s = blockIdx.x + i * gridDim.x;
+#pragma unroll
+    for (int p = 0; p < NP; p++) {
+      const qm31 hs = tables[p * per + lo_n + s];  // the same for the whole CTA
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int l = 0; l < 4; l++) acc[p][j][l] += (uint64_t)x[j] * hs.v[l];
+    }
+    if (i % 3 == 2) {  // at most three products since the last fold
+#pragma unroll
+      for (int p = 0; p < NP; p++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+          for (int l = 0; l < 4; l++) acc[p][j][l] = ev_fold(acc[p][j][l]);
+    }
+  }
+  cp_async_wait_grp<0>();
+  qm31 tot[NP];
+#pragma unroll
+  for (int p = 0; p < NP; p++) {
+    tot[p] = qzero();
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const qm31 part{{ev_reduce(acc[p][j][0]), ev_reduce(acc[p][j][1]), ev_reduce(acc[p][j][2]),
+                       ev_reduce(acc[p][j][3])}};
+      tot[p] = qadd(tot[p], qmul(part, tables[p * per + 4 * threadIdx.x + j]));
     }
   }
   __shared__ uint32_t red[EV_THREADS / 32][NP * 4];
@@ -415,9 +540,17 @@ int eval_at_points(const uint32_t* const* h_cols, uint32_t n_cols, uint32_t L, c
   basis_table_kernel<<<blocks_for((uint64_t)np * per, 256), 256, 0, st>>>(mp, np, hb, lo_n, hi_n, tables);
   VS_LAUNCHED("basis_table_kernel");
   const dim3 grid(gx, n_cols);
-  if (np == 1) eval_points_kernel<1><<<grid, EV_THREADS, 0, st>>>(d_cols, hb, lo_n, hi_n, tables, partials);
-  else eval_points_kernel<2><<<grid, EV_THREADS, 0, st>>>(d_cols, hb, lo_n, hi_n, tables, partials);
-  VS_LAUNCHED("eval_points_kernel");
+  bool ring = hb == EV_LOG_SEG && hi_n >= 4;
+  for (uint32_t c = 0; c < n_cols; c++) ring = ring && (reinterpret_cast<uintptr_t>(h_cols[c]) & 15) == 0;
+  if (ring) {
+    if (np == 1) eval_points_ring_kernel<1><<<grid, EV_THREADS, 0, st>>>(d_cols, lo_n, hi_n, tables, partials);
+    else eval_points_ring_kernel<2><<<grid, EV_THREADS, 0, st>>>(d_cols, lo_n, hi_n, tables, partials);
+    VS_LAUNCHED("eval_points_ring_kernel");
+  } else {
+    if (np == 1) eval_points_kernel<1><<<grid, EV_THREADS, 0, st>>>(d_cols, hb, lo_n, hi_n, tables, partials);
+    else eval_points_kernel<2><<<grid, EV_THREADS, 0, st>>>(d_cols, hb, lo_n, hi_n, tables, partials);
+    VS_LAUNCHED("eval_points_kernel");
+  }
   std::vector<uint32_t> hp((uint64_t)n_cols * gx * np * 4);
   VS_CUDA(cudaMemcpyAsync(hp.data(), partials, hp.size() * 4, cudaMemcpyDeviceToHost, st));
   VS_CUDA(cudaStreamSynchronize(st));
