@@ -230,6 +230,56 @@ def oods_quotients(args, V, torch, lde, N, st, ev):
     return res
 
 
+def fold_dropins(args, V, torch, fri_src, ev):
+    """The reference's plain FRI fold kernels (no commitment) on the step's QM31
+    vector: cuda_fold_circle_into_line_soa of 2^k values into an accumulated line of
+    2^(k-1) (fri.cu:44-78), then cuda_fold_line_soa of that line (fri.cu:10-39).
+    Algorithmic bytes: circle 16N read + 2N twiddles + 8N accumulator read + 8N
+    written; line fold of m values 16m + 2m + 8m. CUDA-event time, default stream."""
+    L = V.lib()
+    N = fri_src.shape[1]
+    half = N // 2
+    dev = lambda words: torch.empty(words, dtype=torch.int32, device="cuda")  # noqa: E731
+
+    def seeded(words, seed):
+        t = dev(words)
+        V.check(L.vs_fill_uniform_m31(t.data_ptr(), words, seed, 0, None))
+        return t
+
+    tw_c, tw_l = seeded(half, SEED + 20), seeded(half // 2, SEED + 21)  # stand-in twiddles (value-independent cost)
+    line = [seeded(half, SEED + 22 + k) for k in range(4)]
+    out = [dev(half // 2) for _ in range(4)]
+    alpha = (C.c_uint32 * 4)(1, 2, 3, 4)
+    alpha_sq = (C.c_uint32 * 4)(5, 6, 7, 8)
+    src = [fri_src[k].data_ptr() for k in range(4)]
+
+    def circle():
+        L.cuda_fold_circle_into_line_soa(*[x.data_ptr() for x in line], *src, tw_c.data_ptr(), alpha, alpha_sq, half)
+
+    def fold_line():
+        L.cuda_fold_line_soa(*[x.data_ptr() for x in line], tw_l.data_ptr(), *[o.data_ptr() for o in out], alpha,
+                             half // 2)
+
+    hbm = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0)) \
+        if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
+    res = {}
+    for name, fn, alg in (("fold_circle_into_line", circle, 34 * N), ("fold_line", fold_line, 26 * half)):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        s0 = torch.cuda.default_stream()
+        e0.record(s0)
+        for _ in range(args.steps):
+            fn()
+        e1.record(s0)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        res[name] = {"ms": ms, "algorithmic_bytes": alg, "achieved_gbs": alg / (ms / 1e3) / 1e9,
+                     "hbm_frac": alg / (ms / 1e3) / 1e9 / hbm}
+    res["workload"] = f"circle fold 2^{N.bit_length() - 1} -> 2^{half.bit_length() - 1}, line fold of 2^{half.bit_length() - 1}"
+    return res
+
+
 # ---------------------------------------------------------------- Cairo trace chain
 def cairo_chain(args, V, torch, ev):
     """The reference Cairo prover's commitment chain at production width, on the
@@ -515,6 +565,7 @@ def main():
              "row_packed_root_ms": phase["merkle"]}
 
     oods = oods_quotients(args, V, torch, lde, N, st, ev) if rank == 0 and not args.no_oods else None
+    folds = fold_dropins(args, V, torch, fri_src, ev) if rank == 0 and not args.no_oods else None
 
     # End to end through the C ABI from pinned host buffers: every step copies its
     # inputs host -> device and reads its roots back. Inputs are double-buffered on
@@ -607,7 +658,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic (seeded SplitMix64 uniform M31)",
                 "config": config_json(args), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": clk.summary(), "three_tree_commit": three, "oods": oods,
+                "gpu_launches": launches, "clocks": clk.summary(), "three_tree_commit": three, "oods": oods, "fri_fold_dropins": folds,
                 "cairo": cairo, "proofs": proofs}
         print(json.dumps(line), flush=True)
     replicas.finalize()

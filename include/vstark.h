@@ -176,6 +176,28 @@ void cuda_m31_add(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t 
 void cuda_m31_mul(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n);
 void cuda_device_sync(void);
 
+/* --- kernels behind the stwo Backend adapter (crates/cuda-backend) ---
+ * All device pointers; asynchronous on the default stream unless noted. */
+/* dst[i] = src[idx[i]] for i < n (src/cuda/ffi.rs:812; cuda/gather.cu:44-53;
+ * caller crates/cuda-backend/src/column.rs:489). */
+void cuda_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint32_t n);
+/* dst[8i .. 8i+8) = src[8 idx[i] .. 8 idx[i]+8): 32-byte hashes (src/cuda/ffi.rs:816;
+ * cuda/gather.cu:55-64; caller column.rs:504). */
+void cuda_gather_u256(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint32_t n);
+/* Partial sums of sum_i evals[i] * weights[i] (M31 times QM31, weights 4 words per
+ * element): out[4b .. 4b+4) is the sum over the 256-element chunks c with
+ * c mod n_blocks == b; the caller adds the n_blocks partials. Synchronises the device
+ * (src/cuda/ffi.rs:828-834; cuda/barycentric_eval.cu:84-95; caller poly_ops.rs:332). */
+void cuda_barycentric_eval(const uint32_t* evals, const uint32_t* weights, uint32_t n, uint32_t* out,
+                           uint32_t n_blocks);
+/* In place, QM31 elements of 4 words: col[i] += curr[((i >> (log_ratio+1)) << 1) | (i & 1)]
+ * for i < col_n (src/cuda/ffi.rs:958; cuda/accumulate_lift.cu:41-50). */
+void cuda_accumulate_lift(uint32_t* col, const uint32_t* curr, uint32_t col_n, uint32_t log_ratio);
+/* output_col_ptrs[16c + p][g] = input_col_ptrs[c][16g + p] for c < 4, p < 16; both are
+ * device arrays of device pointers (4 and 64 of them) (src/cuda/ffi.rs:960-964;
+ * cuda/pack_leaves.cu:44-52; caller merkle_ops.rs:193). */
+void cuda_pack_leaves(const uint32_t* const* input_col_ptrs, uint32_t* const* output_col_ptrs, uint32_t n);
+
 /* ===================================================================== */
 /* 2. vs_* entry points (no reference counterpart)                        */
 /* ===================================================================== */

@@ -15,7 +15,8 @@ if [ ! -d "$REF_ROOT/cuda" ]; then
 fi
 mkdir -p "$OUT"
 SRCS="circle_ntt.cu circle_ntt_stwo.cu twiddles.cu batch_inverse.cu blake2s.cu merkle_leaves_lifted.cu
-      fri.cu constraint.cu quotient.cu bit_reverse_wide.cu fields.cu"
+      fri.cu constraint.cu quotient.cu bit_reverse_wide.cu fields.cu gather.cu barycentric_eval.cu
+      accumulate_lift.cu pack_leaves.cu"
 OBJS=""
 for s in $SRCS; do
   o="$OUT/${s%.cu}.o"

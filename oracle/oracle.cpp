@@ -1027,6 +1027,35 @@ bool deserialize_proof(const uint8_t* data, size_t len, StarkProof& p) {
   return r.ok && r.pos == len;
 }
 
+// ------------------------------------------------------------------ stwo Backend adapter kernels
+void gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint64_t n) {
+  for (uint64_t i = 0; i < n; i++) dst[i] = src[idx[i]];
+}
+void gather_u256(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint64_t n) {
+  for (uint64_t i = 0; i < n; i++)
+    for (int k = 0; k < 8; k++) dst[8 * i + k] = src[8 * (uint64_t)idx[i] + k];
+}
+void barycentric_partials(const uint32_t* evals, const uint32_t* weights, uint64_t n, uint32_t n_blocks, uint32_t* out) {
+  std::vector<QM31> part(n_blocks, QM31{{0, 0, 0, 0}});
+  for (uint64_t i = 0; i < n; i++) {
+    QM31 w{{weights[4 * i], weights[4 * i + 1], weights[4 * i + 2], weights[4 * i + 3]}};
+    QM31& acc = part[(i / 256) % n_blocks];
+    acc = qm_add(acc, qm_scale(w, evals[i]));  // qm31_mul_m31: each limb times the M31 value
+  }
+  for (uint32_t b = 0; b < n_blocks; b++) std::memcpy(out + 4 * (uint64_t)b, part[b].v, 16);
+}
+void accumulate_lift(uint32_t* col, const uint32_t* curr, uint64_t col_n, uint32_t log_ratio) {
+  const uint32_t shift = log_ratio + 1;
+  for (uint64_t i = 0; i < col_n; i++) {
+    uint64_t s = ((shift >= 64 ? 0 : (i >> shift)) << 1) | (i & 1);
+    for (int k = 0; k < 4; k++) col[4 * i + k] = m31_add(col[4 * i + k], curr[4 * s + k]);
+  }
+}
+void pack_leaves(const uint32_t* const in[4], uint32_t* const out[64], uint64_t n) {
+  for (uint32_t c = 0; c < 4; c++)
+    for (uint64_t k = 0; k < n; k++) out[16 * c + (k % 16)][k / 16] = in[c][k];
+}
+
 // ------------------------------------------------------------------ Cairo group commitment
 uint32_t coset_vanishing_at(const Coset& c, CPoint p) {  // circle.rs:238-253
   const CPoint shp = cp_repeated_double(CP_GENERATOR, 30 - c.log_size);

@@ -294,6 +294,19 @@ std::string verify(const StarkProof& p);
 std::vector<uint8_t> serialize_proof(const StarkProof& p);
 bool deserialize_proof(const uint8_t* data, size_t len, StarkProof& out);
 
+// ---------------------------------------------------------------- stwo Backend adapter kernels
+// gather.cu:10-18: dst[i] = src[idx[i]]
+void gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint64_t n);
+// gather.cu:22-40: dst[8i..8i+8) = src[8 idx[i] .. 8 idx[i]+8)
+void gather_u256(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint64_t n);
+// barycentric_eval.cu:30-83 with 256 threads per block: out[4b..4b+4) = sum of
+// evals[i] * weights[i] (QM31 weights, 4 words each) over i with (i / 256) mod n_blocks == b.
+void barycentric_partials(const uint32_t* evals, const uint32_t* weights, uint64_t n, uint32_t n_blocks, uint32_t* out);
+// accumulate_lift.cu:16-37: col[i] += curr[((i >> (log_ratio + 1)) << 1) | (i & 1)], QM31 elements of 4 words.
+void accumulate_lift(uint32_t* col, const uint32_t* curr, uint64_t col_n, uint32_t log_ratio);
+// pack_leaves.cu:22-38: out[16c + p][j] = in[c][16j + p] for every input word 16j + p < n.
+void pack_leaves(const uint32_t* const in[4], uint32_t* const out[64], uint64_t n);
+
 // ---------------------------------------------------------------- seeded inputs
 // SplitMix64; uniform M31 = (u64 >> 33) rejecting P.
 struct SplitMix64 {

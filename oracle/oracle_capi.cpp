@@ -462,3 +462,26 @@ extern "C" void oracle_tree_paths(uint32_t kind, const uint32_t* cols, uint32_t 
     for (size_t k = 0; k < p.size(); k++) put_hash(out_paths + ((uint64_t)q * log_n + k) * 8, p[k]);
   }
 }
+
+// stwo Backend adapter kernels (gather.cu, barycentric_eval.cu, accumulate_lift.cu, pack_leaves.cu).
+extern "C" void oracle_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint64_t n) {
+  gather_u32(src, idx, dst, n);
+}
+extern "C" void oracle_gather_u256(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint64_t n) {
+  gather_u256(src, idx, dst, n);
+}
+extern "C" void oracle_barycentric_partials(const uint32_t* evals, const uint32_t* weights, uint64_t n,
+                                            uint32_t n_blocks, uint32_t* out) {
+  barycentric_partials(evals, weights, n, n_blocks, out);
+}
+extern "C" void oracle_accumulate_lift(uint32_t* col, const uint32_t* curr, uint64_t col_n, uint32_t log_ratio) {
+  accumulate_lift(col, curr, col_n, log_ratio);
+}
+// in_flat: 4 columns of n words back to back; out_flat: 64 columns of out_len words.
+extern "C" void oracle_pack_leaves(const uint32_t* in_flat, uint64_t n, uint32_t* out_flat, uint64_t out_len) {
+  const uint32_t* in[4];
+  uint32_t* out[64];
+  for (int c = 0; c < 4; c++) in[c] = in_flat + c * n;
+  for (int c = 0; c < 64; c++) out[c] = out_flat + c * out_len;
+  pack_leaves(in, out, n);
+}

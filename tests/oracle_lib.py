@@ -479,3 +479,47 @@ def verify(proof: bytes):
     err = C.create_string_buffer(256)
     rc = lib().oracle_verify(ptr(a), C.c_uint64(a.size), err, C.c_uint64(256))
     return rc, err.value.decode()
+
+
+# --- stwo Backend adapter kernels (gather.cu, barycentric_eval.cu, accumulate_lift.cu, pack_leaves.cu)
+def gather_u32(src: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    src = np.ascontiguousarray(src, np.uint32)
+    idx = np.ascontiguousarray(idx, np.uint32)
+    out = np.zeros(max(idx.size, 1), np.uint32)
+    lib().oracle_gather_u32(ptr(src), ptr(idx), ptr(out), C.c_uint64(idx.size))
+    return out[: idx.size]
+
+
+def gather_u256(src: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    src = np.ascontiguousarray(src, np.uint32)
+    idx = np.ascontiguousarray(idx, np.uint32)
+    out = np.zeros(max(8 * idx.size, 1), np.uint32)
+    lib().oracle_gather_u256(ptr(src), ptr(idx), ptr(out), C.c_uint64(idx.size))
+    return out[: 8 * idx.size]
+
+
+def barycentric_partials(evals: np.ndarray, weights: np.ndarray, n_blocks: int) -> np.ndarray:
+    """(n_blocks, 4) partial sums; weights are QM31 AoS (4 words per element)."""
+    evals = np.ascontiguousarray(evals, np.uint32)
+    weights = np.ascontiguousarray(weights, np.uint32)
+    out = np.zeros((max(n_blocks, 1), 4), np.uint32)
+    lib().oracle_barycentric_partials(ptr(evals), ptr(weights), C.c_uint64(evals.size), C.c_uint32(n_blocks), ptr(out))
+    return out[:n_blocks]
+
+
+def accumulate_lift(col: np.ndarray, curr: np.ndarray, log_ratio: int) -> np.ndarray:
+    """col (col_n*4 words, QM31 AoS) after col[i] += curr[src(i)]; returns a new array."""
+    col = np.ascontiguousarray(col, np.uint32).copy()
+    curr = np.ascontiguousarray(curr, np.uint32)
+    lib().oracle_accumulate_lift(ptr(col), ptr(curr), C.c_uint64(col.size // 4), C.c_uint32(log_ratio))
+    return col
+
+
+def pack_leaves(cols: np.ndarray) -> np.ndarray:
+    """cols (4, n) -> (64, ceil(n/16)); words past the end of a short last group stay 0."""
+    cols = np.ascontiguousarray(cols, np.uint32)
+    n = cols.shape[1]
+    out_len = (n + 15) // 16
+    out = np.zeros((64, max(out_len, 1)), np.uint32)
+    lib().oracle_pack_leaves(ptr(cols), C.c_uint64(n), ptr(out), C.c_uint64(max(out_len, 1)))
+    return out[:, :out_len]

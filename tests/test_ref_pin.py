@@ -220,3 +220,40 @@ def test_bit_reverse(R):
     d = dev(x)
     R.cuda_bit_reverse_m31(C.c_void_p(ptr(d)), C.c_uint32(12))
     assert np.array_equal(host(d), O.bit_reverse(x, 12))
+
+
+def test_adapter_kernels(R):
+    """cuda/gather.cu, barycentric_eval.cu, accumulate_lift.cu, pack_leaves.cu against the oracle."""
+    rng = np.random.default_rng(3)
+    src = rand_m31(rng, 8 * 600)
+    idx = rng.integers(0, 600, size=500).astype(np.uint32)
+    out = zeros(500)
+    R.cuda_gather_u32(C.c_void_p(ptr(dev(src))), C.c_void_p(ptr(dev(idx))), C.c_void_p(ptr(out)), C.c_uint32(500))
+    assert np.array_equal(host(out), O.gather_u32(src, idx))
+    out8 = zeros(8 * 500)
+    R.cuda_gather_u256(C.c_void_p(ptr(dev(src))), C.c_void_p(ptr(dev(idx))), C.c_void_p(ptr(out8)), C.c_uint32(500))
+    assert np.array_equal(host(out8), O.gather_u256(src, idx))
+
+    for n, n_blocks in [(1000, 4), (70000, 256), (300, 3)]:
+        e = rand_m31(rng, n)
+        w = rand_m31(rng, 4 * n)
+        part = zeros(4 * n_blocks)
+        R.cuda_barycentric_eval(C.c_void_p(ptr(dev(e))), C.c_void_p(ptr(dev(w))), C.c_uint32(n), C.c_void_p(ptr(part)),
+                                C.c_uint32(n_blocks))
+        assert np.array_equal(host(part).reshape(n_blocks, 4), O.barycentric_partials(e, w, n_blocks))
+
+    for log_col, log_curr in [(1, 1), (8, 3), (12, 11)]:
+        col = rand_m31(rng, 4 << log_col)
+        curr = rand_m31(rng, 4 << log_curr)
+        d = dev(col)
+        R.cuda_accumulate_lift(C.c_void_p(ptr(d)), C.c_void_p(ptr(dev(curr))), C.c_uint32(1 << log_col),
+                               C.c_uint32(log_col - log_curr))
+        assert np.array_equal(host(d), O.accumulate_lift(col, curr, log_col - log_curr))
+
+    for n in (4096, 40):
+        cols = rand_m31(rng, 4, n)
+        outs = [zeros((n + 15) // 16) for _ in range(64)]
+        R.cuda_pack_leaves(C.c_void_p(ptr(ptr_array([dev(c) for c in cols]))), C.c_void_p(ptr(ptr_array(outs))),
+                           C.c_uint32(n))
+        sync()
+        assert np.array_equal(np.stack([host(o) for o in outs]), O.pack_leaves(cols))
