@@ -19,10 +19,12 @@
 // HBM round trips instead of the reference's 24 per-layer launches.
 //
 // The LDE path fuses interpolate -> zero-pad -> evaluate: the top pass of the
-// inverse transform keeps the coefficients in registers and directly runs the
+// inverse transform keeps the coefficients in shared memory and directly runs the
 // forward top pass for each of the 2^B blowup blocks (the top B forward layers
 // of a zero-padded input only replicate the coefficients), so neither the
-// coefficients nor the zero padding touch HBM.
+// coefficients nor the zero padding touch HBM. Its upper-tile form works on
+// 16-byte chunks in three-layer rounds (128-bit shared-memory traffic, one
+// twiddle per chunk, 80 registers, three CTAs per SM).
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -345,7 +347,9 @@ __device__ __forceinline__ void rounds_below_top(uint32_t* sm, const TileGeo& g,
 // Fused LDE top pass: inverse layers [a, l-1] of the trace tile with the 1/n
 // scale; the coefficients are parked in a second shared tile, and for each
 // blowup block q the forward layers [a, l-1] of the evaluation domain (tile
-// prefix hi = q) run on them and the result is written to dst block q.
+// prefix hi = q) run on them and the result is written to dst block q. This
+// five-layer-round form serves C = 0 tiles (transforms of at most 13 layers);
+// upper tiles (C >= 2) use the chunk-round form ntt_lde_top4_kernel below.
 template <int M, int C>
 __global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_lde_top_kernel(NttPass inv, NttPass fwd, uint32_t B) {
   using S = Tile<M, C>;
@@ -382,6 +386,196 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_lde_top_kernel(NttPas
   }
 }
 
+// ---- Chunk-round variant of the fused LDE top pass (tiles with C >= 2).
+// A thread holds eight 16-byte chunks (the four words of tile bits 0-1) along
+// three round bits, so every shared-memory access is 128-bit, and the four words
+// of a chunk share each twiddle (7 twiddles per three-layer round instead of 31
+// per five-layer round). Round r covers tile bits [C + 3r, C + 3r + R(r)).
+// The tile uses swz<0> (chunk index XOR word bits 5-7), which keeps every
+// quarter-warp of these 128-bit accesses on eight distinct chunk positions for
+// every round shape with C >= 2 (round bits at or above word bit 2).
+template <int M, int C>
+struct Tile4 {
+  static_assert(C >= 2, "chunk rounds need at least two contiguous index bits");
+  static constexpr int T = M + C, NT = 1 << (T - 5), SIZE = 1 << T, NR = (M + 2) / 3;
+  static constexpr int P0(int r) { return C + 3 * r; }
+  static constexpr int R(int r) { return 3 * (r + 1) <= M ? 3 : M - 3 * r; }
+};
+
+// Word address of chunk k (R round bits at word bit P0) of chunk group o; o
+// enumerates the chunk-index bits outside the round.
+template <int P0, int R>
+__device__ __forceinline__ uint32_t ins4(uint32_t o, uint32_t k) {
+  constexpr int Q = P0 - 2;
+  return (((o >> Q) << (Q + R)) | (k << Q) | (o & ((1u << Q) - 1))) << 2;
+}
+
+template <int M, int C>
+__device__ __forceinline__ void tile_load4(uint32_t* sm, const uint32_t* __restrict__ src, const TileGeo& g,
+                                           uint32_t mask) {
+  using S = Tile4<M, C>;
+#pragma unroll
+  for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
+    const uint32_t e = 4 * (threadIdx.x + i * S::NT);
+    *reinterpret_cast<uint4*>(sm + swz<0>(e)) = *reinterpret_cast<const uint4*>(src + (gidx<M, C>(g, e) & mask));
+  }
+}
+template <int M, int C>
+__device__ __forceinline__ void tile_store4(const uint32_t* sm, uint32_t* __restrict__ dst, const TileGeo& g) {
+  using S = Tile4<M, C>;
+#pragma unroll
+  for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
+    const uint32_t e = 4 * (threadIdx.x + i * S::NT);
+    *reinterpret_cast<uint4*>(dst + gidx<M, C>(g, e)) = *reinterpret_cast<const uint4*>(sm + swz<0>(e));
+  }
+}
+
+template <int M, int C, int r>
+__device__ __forceinline__ void rload4(uint4 (&v)[8], const uint32_t* sm) {
+  using S = Tile4<M, C>;
+  constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (3 - R);
+#pragma unroll
+  for (int s = 0; s < SUB; s++)
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      v[s * K + k] = *reinterpret_cast<const uint4*>(sm + swz<0>(ins4<P0, R>(threadIdx.x + s * S::NT, k)));
+}
+template <int M, int C, int r>
+__device__ __forceinline__ void rstore4(const uint4 (&v)[8], uint32_t* sm) {
+  using S = Tile4<M, C>;
+  constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (3 - R);
+#pragma unroll
+  for (int s = 0; s < SUB; s++)
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      *reinterpret_cast<uint4*>(sm + swz<0>(ins4<P0, R>(threadIdx.x + s * S::NT, k))) = v[s * K + k];
+}
+
+template <bool FWD>
+__device__ __forceinline__ void bfly4(uint4& a, uint4& b, uint32_t tt) {
+  bfly<FWD>(a.x, b.x, tt);
+  bfly<FWD>(a.y, b.y, tt);
+  bfly<FWD>(a.z, b.z, tt);
+  bfly<FWD>(a.w, b.w, tt);
+}
+
+// Butterflies of chunk round r; layer q of the round (tile bit p = P0 + q) is
+// global layer a + p - C with group index h = hi * 2^(T-1-p) + (address >> (p+1)).
+// Twiddle tables are 16-byte aligned up to their size (host-checked), as for rbfly.
+template <bool FWD, int M, int C, int r>
+__device__ __forceinline__ void rbfly4(uint4 (&v)[8], const TileGeo& g, const NttTw& tw) {
+  using S = Tile4<M, C>;
+  constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (3 - R), T = S::T;
+#pragma unroll
+  for (int s = 0; s < SUB; s++) {
+    const uint32_t base = ins4<P0, R>(threadIdx.x + s * S::NT, 0);
+    uint32_t t[K];  // layer q's twiddles at t[K - (K >> q) + gg]
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+      const int p = P0 + q;
+      const uint32_t hb = (g.hi << (T - 1 - p)) | (base >> (p + 1));
+      const uint32_t* tp = tw.layer[g.a + p - C] + hb;
+      const int cnt = K >> (q + 1), o = K - (K >> q);
+      if (cnt == 4) {
+        const uint4 w = __ldg(reinterpret_cast<const uint4*>(tp));
+        t[o] = w.x << 1;
+        t[o + 1] = w.y << 1;
+        t[o + 2] = w.z << 1;
+        t[o + 3] = w.w << 1;
+      } else if (cnt == 2) {
+        const uint2 w = __ldg(reinterpret_cast<const uint2*>(tp));
+        t[o] = w.x << 1;
+        t[o + 1] = w.y << 1;
+      } else {
+        t[o] = __ldg(tp) << 1;
+      }
+    }
+#pragma unroll
+    for (int qq = 0; qq < R; qq++) {
+      const int q = FWD ? R - 1 - qq : qq;
+#pragma unroll
+      for (int gg = 0; gg < (K >> (q + 1)); gg++) {
+        const uint32_t tv = t[K - (K >> q) + gg];
+#pragma unroll
+        for (int l = 0; l < (1 << q); l++) {
+          const int k0 = (gg << (q + 1)) | l;
+          bfly4<FWD>(v[s * K + k0], v[s * K + k0 + (1 << q)], tv);
+        }
+      }
+    }
+  }
+}
+
+template <bool FWD, int M, int C, int r>
+__device__ __forceinline__ void round4(uint32_t* sm, const TileGeo& g, const NttTw& tw) {
+  uint4 v[8];
+  rload4<M, C, r>(v, sm);
+  rbfly4<FWD, M, C, r>(v, g, tw);
+  rstore4<M, C, r>(v, sm);
+}
+// Rounds [lo, hi] in transform order (forward: hi down to lo), barrier after each.
+template <bool FWD, int M, int C>
+__device__ __forceinline__ void rounds4(uint32_t* sm, const TileGeo& g, const NttTw& tw, int lo, int hi) {
+  using S = Tile4<M, C>;
+#pragma unroll
+  for (int i = 0; i < S::NR; i++) {
+    const int r = FWD ? S::NR - 1 - i : i;
+    if (r < lo || r > hi) continue;
+    switch (r) {
+      case 0: round4<FWD, M, C, 0>(sm, g, tw); break;
+      case 1: round4<FWD, M, C, (S::NR > 1 ? 1 : 0)>(sm, g, tw); break;
+      case 2: round4<FWD, M, C, (S::NR > 2 ? 2 : 0)>(sm, g, tw); break;
+      default: round4<FWD, M, C, (S::NR > 3 ? 3 : 0)>(sm, g, tw); break;
+    }
+    __syncthreads();
+  }
+}
+
+// Same dataflow as ntt_lde_top_kernel: inverse rounds with the 1/n scale folded
+// into the last one, which parks the coefficients in the second tile; then for
+// each blowup block q the forward rounds from the parked tile, stored to block q.
+template <int M, int C>
+__global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPass inv, NttPass fwd, uint32_t B) {
+  using S = Tile4<M, C>;
+  static_assert(S::NR <= 4, "at most four chunk rounds");
+  constexpr int TOP = S::NR - 1;
+  extern __shared__ __align__(16) uint32_t lde4_sm[];
+  uint32_t* sm = lde4_sm;            // working tile
+  uint32_t* cf = lde4_sm + S::SIZE;  // coefficients
+  const TileGeo gi = tile_geo<M, C>(inv.a, blockIdx.x);
+  tile_load4<M, C>(sm, col_src(inv, blockIdx.y), gi, inv.src_mask);
+  __syncthreads();
+  rounds4<false, M, C>(sm, gi, inv.tw, 0, TOP - 1);
+  {
+    uint4 v[8];
+    rload4<M, C, TOP>(v, sm);
+    rbfly4<false, M, C, TOP>(v, gi, inv.tw);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      v[k].x = mul(v[k].x, inv.scale);
+      v[k].y = mul(v[k].y, inv.scale);
+      v[k].z = mul(v[k].z, inv.scale);
+      v[k].w = mul(v[k].w, inv.scale);
+    }
+    rstore4<M, C, TOP>(v, cf);
+  }
+  __syncthreads();
+  uint32_t* dst = col_dst(fwd, blockIdx.y);
+  for (uint32_t q = 0; q < (1u << B); q++) {
+    TileGeo gf = gi;
+    gf.hi = q;
+    gf.gbase = (q << (gi.a + M)) | gi.gbase;
+    uint4 v[8];
+    rload4<M, C, TOP>(v, cf);
+    rbfly4<true, M, C, TOP>(v, gf, fwd.tw);
+    rstore4<M, C, TOP>(v, sm);  // the previous block's tile_store finished before the loop-end barrier
+    __syncthreads();
+    rounds4<true, M, C>(sm, gf, fwd.tw, 0, TOP - 1);
+    tile_store4<M, C>(sm, dst, gf);
+    __syncthreads();
+  }
+}
+
 // Launch tables: single / lower passes use C = 0 (T = M, 5 <= M <= 13); upper
 // passes use T = 13 (C = 13 - M, 1 <= M <= 11).
 using PassFn = void (*)(NttPass, uint32_t, uint32_t);
@@ -389,7 +583,7 @@ using TopFn = void (*)(NttPass, NttPass, uint32_t);
 template <bool FWD, int M> PassFn pass_lo() { return ntt_pass_kernel<FWD, M, 0>; }
 template <bool FWD, int M> PassFn pass_hi() { return ntt_pass_kernel<FWD, M, 13 - M>; }
 template <int M> TopFn top_lo() { return ntt_lde_top_kernel<M, 0>; }
-template <int M> TopFn top_hi() { return ntt_lde_top_kernel<M, 13 - M>; }
+template <int M> TopFn top_hi() { return ntt_lde_top4_kernel<M, 13 - M>; }
 
 static PassFn pass_fn(bool fwd, uint32_t M, uint32_t C) {
 #define VS_LO(m) case m: return fwd ? pass_lo<true, m>() : pass_lo<false, m>();
