@@ -462,6 +462,9 @@ def main():
     ap.add_argument("--cairo-log-n", type=int, default=22, help="trace rows (log) of the Cairo chain")
     ap.add_argument("--slots", type=int, default=8, help="concurrent slots of the batched and served engines")
     ap.add_argument("--served-jobs", type=int, default=600)
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default NTT plans (no autotuning)")
+    ap.add_argument("--tune-sizes", type=int, nargs="*", default=list(range(16, 25)),
+                    help="trace sizes (log) the NTT autotuner tunes before the timed runs")
     ap.add_argument("--prove-sizes", type=int, nargs="*", default=[20, 24, 28],
                     help="log_n of the single-proof latency runs")
     args = ap.parse_args()
@@ -484,6 +487,19 @@ def main():
     # The stream-ordered pool keeps what it has allocated, as the reference's own
     # benchmark sets it (init_memory_pool_greedy, src/bin/full_benchmark.rs:23).
     api.init_memory_pool((1 << 64) - 1)
+
+    # NTT launch shapes per size chosen by the autotuner before anything is timed
+    # (34-column stwo LDEs); every later transform of a tuned size uses its plan.
+    tuning = None
+    if not args.no_autotune:
+        tuning = {}
+        for tl in sorted(set(args.tune_sizes) | {args.log_n}):
+            default = api.ntt_plan(tl)
+            r = api.autotune_lde(tl, n_cols=args.cols, blowup=2, reps=3)
+            times = dict(r["candidates"])
+            tuning[str(tl)] = {"plan": list(r["best"]), "ms": times[tuple(r["best"])],
+                               "default_plan": list(default), "default_ms": times.get(tuple(default)),
+                               "candidates": len(times)}
 
     n_cols, log_n, blow, fri_log, N, committed = workload(args)
     n = 1 << log_n
@@ -658,7 +674,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic (seeded SplitMix64 uniform M31)",
                 "config": config_json(args), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": clk.summary(), "three_tree_commit": three, "oods": oods, "fri_fold_dropins": folds,
+                "gpu_launches": launches, "clocks": clk.summary(), "three_tree_commit": three, "oods": oods, "fri_fold_dropins": folds, "ntt_autotune": tuning,
                 "cairo": cairo, "proofs": proofs}
         print(json.dumps(line), flush=True)
     replicas.finalize()

@@ -220,6 +220,30 @@ int vs_lde_stwo(const uint32_t* d_src, uint64_t src_stride, uint32_t* d_dst, uin
 int vs_lde_native(const uint32_t* d_src, uint64_t src_stride, uint32_t* d_dst, uint64_t dst_stride, uint32_t n_cols,
                   uint32_t log_n, uint32_t blowup_bits, vs_stream_t stream);
 
+/* NTT launch-shape autotuner (no counterpart in the reference, which launches one
+ * kernel per butterfly layer). A plan per transform size log_n (process wide, used
+ * by every NTT and LDE of that size, native and stwo; an LDE uses the plan of its
+ * trace size):
+ *   lower      layers of the first (lower) pass; 14 <= log_n <= 24 accepts
+ *              max(5, log_n - 11) .. 13, other sizes only their default
+ *              (13, or log_n below 14);
+ *   items      tiles a pass CTA transforms before it retires, 1..64 (0: 8);
+ *   top_radix  layers per register round of the LDE top pass above 13 layers:
+ *              3 (16-byte chunks, the default) or 5 (words); 0: default.
+ * Plans change only how layers are grouped into launches; results are identical.
+ * vs_ntt_plan_set(log_n, 0, 0, 0) restores the defaults. */
+int vs_ntt_plan_set(uint32_t log_n, uint32_t lower, uint32_t items, uint32_t top_radix);
+int vs_ntt_plan_get(uint32_t log_n, uint32_t* lower, uint32_t* items, uint32_t* top_radix);
+/* The plans the autotuner tries for log_n, 3 words each (lower, items, top_radix);
+ * *n_out = their number (host only, no device calls). */
+int vs_ntt_plan_candidates(uint32_t log_n, uint32_t* out, uint32_t cap, uint32_t* n_out);
+/* Times every candidate plan on an n_cols-column stwo LDE of 2^log_n rows (seeded
+ * columns, one warm-up and `reps` timed runs each, CUDA events on `stream`), keeps the
+ * fastest as the plan of log_n and writes it to best[3]; ms[i] (i < cap) receives
+ * candidate i's time per LDE. Allocates its scratch columns on `stream`. */
+int vs_autotune_lde(uint32_t log_n, uint32_t n_cols, uint32_t blowup_bits, uint32_t reps, uint32_t* best,
+                    float* ms, uint32_t cap, vs_stream_t stream);
+
 /* Merkle root over n_cols columns of 2^log_leaves rows with the row-packed
  * multi-block leaf (all columns, merkle_leaves_lifted.cu semantics with equal
  * sizes). Column c at d_cols + c*stride. root written to d_root (device, 8 words). */

@@ -117,6 +117,51 @@ def init_memory_pool(release_threshold_bytes: int = 2 << 30) -> None:
     check(lib().vs_init_memory_pool(release_threshold_bytes), "vs_init_memory_pool")
 
 
+def ntt_plan(log_n: int) -> tuple[int, int, int]:
+    """(lower pass layers, tiles per CTA, LDE top-pass round layers) used for 2^log_n transforms."""
+    v = [C.c_uint32() for _ in range(3)]
+    check(lib().vs_ntt_plan_get(log_n, *[C.byref(x) for x in v]), "vs_ntt_plan_get")
+    return tuple(int(x.value) for x in v)
+
+
+def set_ntt_plan(log_n: int, lower: int = 0, items: int = 0, top_radix: int = 0) -> None:
+    """Sets the launch shape of 2^log_n transforms (zeros restore the defaults)."""
+    check(lib().vs_ntt_plan_set(log_n, lower, items, top_radix), "vs_ntt_plan_set")
+
+
+def ntt_plan_candidates(log_n: int) -> list[tuple[int, int, int]]:
+    n = C.c_uint32()
+    check(lib().vs_ntt_plan_candidates(log_n, None, 0, C.byref(n)), "vs_ntt_plan_candidates")
+    buf = (C.c_uint32 * max(1, 3 * n.value))()
+    check(lib().vs_ntt_plan_candidates(log_n, buf, n.value, C.byref(n)), "vs_ntt_plan_candidates")
+    return [tuple(buf[3 * i:3 * i + 3]) for i in range(n.value)]
+
+
+def autotune_lde(log_n: int, n_cols: int = 34, blowup: int = 2, reps: int = 3, stream=None) -> dict:
+    """Times every candidate plan of 2^log_n on an n_cols-column LDE, keeps the fastest
+    and returns {"best": plan, "candidates": [(plan, ms per LDE), ...]}."""
+    cands = ntt_plan_candidates(log_n)
+    best = (C.c_uint32 * 3)()
+    ms = (C.c_float * max(1, len(cands)))()
+    check(lib().vs_autotune_lde(log_n, n_cols, blowup, reps, best, ms, len(cands), _stream(stream)),
+          "vs_autotune_lde")
+    return {"best": tuple(best), "candidates": [(c, float(ms[i])) for i, c in enumerate(cands)]}
+
+
+def save_tuning(path, log_ns=range(5, 31)) -> None:
+    """Writes the current plans as JSON ({log_n: [lower, items, top_radix]})."""
+    import json
+    with open(path, "w") as f:
+        json.dump({str(l): list(ntt_plan(l)) for l in log_ns}, f, indent=1)
+
+
+def load_tuning(path) -> None:
+    import json
+    with open(path) as f:
+        for k, v in json.load(f).items():
+            set_ntt_plan(int(k), *v)
+
+
 def launch_count() -> int:
     return int(lib().vs_launch_count())
 

@@ -584,6 +584,7 @@ template <bool FWD, int M> PassFn pass_lo() { return ntt_pass_kernel<FWD, M, 0>;
 template <bool FWD, int M> PassFn pass_hi() { return ntt_pass_kernel<FWD, M, 13 - M>; }
 template <int M> TopFn top_lo() { return ntt_lde_top_kernel<M, 0>; }
 template <int M> TopFn top_hi() { return ntt_lde_top4_kernel<M, 13 - M>; }
+template <int M> TopFn top5_hi() { return ntt_lde_top_kernel<M, 13 - M>; }
 
 static PassFn pass_fn(bool fwd, uint32_t M, uint32_t C) {
 #define VS_LO(m) case m: return fwd ? pass_lo<true, m>() : pass_lo<false, m>();
@@ -597,9 +598,9 @@ static PassFn pass_fn(bool fwd, uint32_t M, uint32_t C) {
 #undef VS_HI
   return nullptr;
 }
-static TopFn top_fn(uint32_t M, uint32_t C) {
+static TopFn top_fn(uint32_t M, uint32_t C, uint32_t radix) {
 #define VS_LO(m) case m: return top_lo<m>();
-#define VS_HI(m) case m: return top_hi<m>();
+#define VS_HI(m) case m: return radix == 5 ? top5_hi<m>() : top_hi<m>();
   if (C == 0) {
     switch (M) { VS_LO(5) VS_LO(6) VS_LO(7) VS_LO(8) VS_LO(9) VS_LO(10) VS_LO(11) VS_LO(12) VS_LO(13) default: break; }
   } else if (M + C == 13) {
@@ -645,10 +646,54 @@ __global__ void scale_kernel(uint32_t* __restrict__ d, uint32_t s, uint32_t n) {
 static const uint32_t kMaxT = 13;  // tile of 8192 words (32 KiB), 256 threads
 static const uint32_t kMinC = 2;   // >= 16-byte contiguous runs per tile row
 
-std::vector<PassRange> plan_passes(uint32_t L) {
+// Per-size plans (process wide). Sizes 14..24 may move layers between the lower
+// pass and the single upper pass: lower in [max(5, L - 11), 13] keeps the upper
+// pass at most 11 layers on a 13-bit tile.
+static std::mutex g_plan_mu;
+static NttPlan g_plan[32];
+
+static bool lower_valid(uint32_t L, uint32_t lower) {
+  if (lower == 0) return true;
+  if (L <= kMaxT || L > 2 * kMaxT - kMinC) return false;
+  return lower >= std::max<uint32_t>(5, L - (kMaxT - kMinC)) && lower <= kMaxT;
+}
+bool ntt_plan_valid(uint32_t L, const NttPlan& p) {
+  return L < 32 && lower_valid(L, p.lower) && p.items <= 64 && (p.top_radix == 0 || p.top_radix == 3 || p.top_radix == 5);
+}
+NttPlan ntt_plan(uint32_t L) {
+  NttPlan p{};
+  if (L < 32) {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    p = g_plan[L];
+  }
+  if (!p.items) p.items = 8;
+  if (!p.top_radix) p.top_radix = 3;
+  return p;
+}
+static void set_plan(uint32_t L, const NttPlan& p) {
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  g_plan[L] = p;
+}
+std::vector<NttPlan> ntt_plan_candidates(uint32_t L) {
+  std::vector<NttPlan> v;
+  std::vector<uint32_t> lowers{0};
+  if (L > kMaxT && L <= 2 * kMaxT - kMinC) {
+    lowers.clear();
+    // lower passes of at least 10 layers (CTAs of 32+ threads); smaller ones are valid but never faster
+    for (uint32_t lo = std::max<uint32_t>(10, L - (kMaxT - kMinC)); lo <= kMaxT; lo++) lowers.push_back(lo);
+  }
+  const bool upper_tile = L > kMaxT;  // the LDE top pass runs on C >= 2 tiles only above 13 layers
+  const std::vector<uint32_t> radices = upper_tile ? std::vector<uint32_t>{3u, 5u} : std::vector<uint32_t>{0u};
+  for (uint32_t lo : lowers)
+    for (uint32_t items : {4u, 8u, 16u})
+      for (uint32_t radix : radices) v.push_back({lo == kMaxT ? 0u : lo, items, radix});
+  return v;
+}
+
+std::vector<PassRange> plan_passes(uint32_t L, uint32_t lower) {
   std::vector<PassRange> v;
   if (L <= kMaxT) { v.push_back({0, L - 1, 0}); return v; }
-  uint32_t lo = kMaxT;
+  uint32_t lo = lower_valid(L, lower) && lower ? lower : kMaxT;
   v.push_back({0, lo - 1, 0});
   uint32_t rem = L - lo, max_u = kMaxT - kMinC;
   uint32_t k = (rem + max_u - 1) / max_u;
@@ -712,7 +757,7 @@ static int launch_pass(NttPass p, bool fwd, uint32_t n_cols, cudaStream_t st) {
   // loads, and CTAs retire every few tens of microseconds, so kernels of
   // higher-priority streams (small jobs beside a large one) get SMs promptly
   // instead of waiting for a whole-GPU persistent kernel to end.
-  constexpr uint64_t kItemsPerCta = 8;
+  const uint64_t kItemsPerCta = p.items ? p.items : 8;
   const uint32_t threads = 1u << (T - 5);
   const uint64_t resident = persistent_grid((const void*)fn, threads, smem);
   const uint32_t grid = (uint32_t)std::min<uint64_t>(total, std::max(resident, (total + kItemsPerCta - 1) / kItemsPerCta));
@@ -848,12 +893,14 @@ static int ntt_transform_aligned(const NttColumns& io, uint32_t L, const NttTw& 
     }
     return VS_OK;
   }
-  auto passes = plan_passes(L);
+  const NttPlan plan = ntt_plan(L);
+  auto passes = plan_passes(L, plan.lower);
   const size_t np = passes.size();
   for (size_t i = 0; i < np; i++) {
     const PassRange& r = fwd ? passes[np - 1 - i] : passes[i];
     NttPass p{};
     p.tw = tw;
+    p.items = plan.items;
     p.log_n = L;
     p.a = r.a;
     p.b = r.b;
@@ -899,12 +946,14 @@ int ntt_lde(const NttColumns& io, uint32_t l, uint32_t B, const NttTw& tw_inv, c
 
 static int ntt_lde_aligned(const NttColumns& io, uint32_t l, uint32_t B, const NttTw& tw_inv, const NttTw& tw_fwd,
                            cudaStream_t st) {
-  auto passes = plan_passes(l);
+  const NttPlan plan = ntt_plan(l);
+  auto passes = plan_passes(l, plan.lower);
   const size_t np = passes.size();
   // 1. inverse passes below the top one: src -> dst[0, n)
   for (size_t i = 0; i + 1 < np; i++) {
     NttPass p{};
     p.tw = tw_inv;
+    p.items = plan.items;
     p.log_n = l;
     p.a = passes[i].a;
     p.b = passes[i].b;
@@ -935,7 +984,7 @@ static int ntt_lde_aligned(const NttColumns& io, uint32_t l, uint32_t B, const N
     pf.dst = io.dst;
     pf.dst_stride = io.dst_stride;
     const uint32_t M = r.b - r.a + 1, T = M + r.c;
-    TopFn fn = top_fn(M, r.c);
+    TopFn fn = top_fn(M, r.c, plan.top_radix);
     if (!fn) return set_error(VS_ERR_INVALID, "ntt: no LDE kernel for shape M=%u C=%u", M, r.c);
     const uint32_t smem = 8u << T;  // working tile + coefficient tile
     VS_TRY(allow_smem((const void*)fn, smem));
@@ -946,6 +995,7 @@ static int ntt_lde_aligned(const NttColumns& io, uint32_t l, uint32_t B, const N
   for (int i = (int)np - 2; i >= 0; i--) {
     NttPass p{};
     p.tw = tw_fwd;
+    p.items = plan.items;
     p.log_n = l + B;
     p.a = passes[i].a;
     p.b = passes[i].b;
@@ -1169,6 +1219,97 @@ int vs_lde_native(const uint32_t* src, uint64_t src_stride, uint32_t* dst, uint6
                   uint32_t log_n, uint32_t blowup, vs_stream_t st) {
   clear_error();
   return lde_cached(TW_NATIVE, src, src_stride, dst, dst_stride, n_cols, log_n, blowup, (cudaStream_t)st);
+}
+
+// ------------------------------------------------------------------ autotuner
+int vs_ntt_plan_set(uint32_t log_n, uint32_t lower, uint32_t items, uint32_t top_radix) {
+  clear_error();
+  // canonical form: the default lower pass (13, or the whole transform up to 13
+  // layers) is 0, and below 14 layers the top pass has only the five-layer form
+  const uint32_t lo = (lower == kMaxT || (log_n <= kMaxT && lower == log_n)) ? 0u : lower;
+  const uint32_t rx = (log_n <= kMaxT && top_radix == 5) ? 0u : top_radix;
+  const NttPlan p{lo, items, rx};
+  if (!ntt_plan_valid(log_n, p))
+    return set_error(VS_ERR_INVALID, "vs_ntt_plan_set: no plan (lower %u, items %u, radix %u) for log_n %u", lower,
+                     items, top_radix, log_n);
+  set_plan(log_n, p);
+  return VS_OK;
+}
+int vs_ntt_plan_get(uint32_t log_n, uint32_t* lower, uint32_t* items, uint32_t* top_radix) {
+  clear_error();
+  if (log_n >= 32 || !lower || !items || !top_radix) return set_error(VS_ERR_INVALID, "vs_ntt_plan_get: bad argument");
+  const NttPlan p = ntt_plan(log_n);
+  *lower = log_n <= kMaxT ? log_n : (p.lower ? p.lower : kMaxT);
+  *items = p.items;
+  *top_radix = log_n <= kMaxT ? 5u : p.top_radix;
+  return VS_OK;
+}
+int vs_ntt_plan_candidates(uint32_t log_n, uint32_t* out, uint32_t cap, uint32_t* n_out) {
+  clear_error();
+  if (log_n >= 32 || !n_out) return set_error(VS_ERR_INVALID, "vs_ntt_plan_candidates: bad argument");
+  const auto v = ntt_plan_candidates(log_n);
+  *n_out = (uint32_t)v.size();
+  for (uint32_t i = 0; i < v.size() && i < cap && out; i++) {
+    out[3 * i] = v[i].lower ? v[i].lower : std::min<uint32_t>(log_n, kMaxT);
+    out[3 * i + 1] = v[i].items;
+    out[3 * i + 2] = v[i].top_radix ? v[i].top_radix : 5u;
+  }
+  return VS_OK;
+}
+
+// Times every candidate plan of log_n on an n_cols-column LDE (stwo convention,
+// seeded columns, `reps` timed runs after one warm-up each, CUDA events on the
+// stream) and keeps the fastest as the plan of log_n.
+int vs_autotune_lde(uint32_t log_n, uint32_t n_cols, uint32_t blowup_bits, uint32_t reps, uint32_t* best,
+                    float* ms_out, uint32_t cap, vs_stream_t stream) {
+  clear_error();
+  cudaStream_t st = (cudaStream_t)stream;
+  if (log_n < 5 || log_n >= 31 || log_n + blowup_bits > 30 || !n_cols || !best)
+    return set_error(VS_ERR_INVALID, "vs_autotune_lde: bad size (log_n %u, blowup %u, cols %u)", log_n, blowup_bits,
+                     n_cols);
+  if (!reps) reps = 3;
+  const uint64_t n = 1ull << log_n, N = n << blowup_bits;
+  const auto cands = ntt_plan_candidates(log_n);
+  const NttPlan saved = [&] {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    return g_plan[log_n];
+  }();
+  uint32_t *src = nullptr, *dst = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = check_cuda(cudaMallocAsync((void**)&src, n * n_cols * 4, st), "vs_autotune_lde alloc");
+  if (rc == VS_OK) rc = check_cuda(cudaMallocAsync((void**)&dst, N * n_cols * 4, st), "vs_autotune_lde alloc");
+  if (rc == VS_OK) rc = vs_fill_uniform_m31(src, n * n_cols, 0x56530007ull, 0, stream);
+  if (rc == VS_OK) rc = check_cuda(cudaEventCreate(&e0), "vs_autotune_lde event");
+  if (rc == VS_OK) rc = check_cuda(cudaEventCreate(&e1), "vs_autotune_lde event");
+  float best_ms = 0.f;
+  NttPlan best_plan = saved;
+  for (size_t i = 0; i < cands.size() && rc == VS_OK; i++) {
+    set_plan(log_n, cands[i]);
+    rc = lde_cached(TW_STWO, src, n, dst, N, n_cols, log_n, blowup_bits, st);
+    if (rc == VS_OK) rc = check_cuda(cudaEventRecord(e0, st), "vs_autotune_lde event");
+    for (uint32_t k = 0; k < reps && rc == VS_OK; k++)
+      rc = lde_cached(TW_STWO, src, n, dst, N, n_cols, log_n, blowup_bits, st);
+    if (rc == VS_OK) rc = check_cuda(cudaEventRecord(e1, st), "vs_autotune_lde event");
+    if (rc == VS_OK) rc = check_cuda(cudaEventSynchronize(e1), "vs_autotune_lde sync");
+    float ms = 0.f;
+    if (rc == VS_OK) rc = check_cuda(cudaEventElapsedTime(&ms, e0, e1), "vs_autotune_lde time");
+    ms /= (float)reps;
+    if (ms_out && i < cap) ms_out[i] = ms;
+    if (rc == VS_OK && (i == 0 || ms < best_ms)) {
+      best_ms = ms;
+      best_plan = cands[i];
+    }
+  }
+  set_plan(log_n, rc == VS_OK ? best_plan : saved);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (src) cudaFreeAsync(src, st);
+  if (dst) cudaFreeAsync(dst, st);
+  if (rc != VS_OK) return rc;
+  best[0] = best_plan.lower ? best_plan.lower : std::min<uint32_t>(log_n, kMaxT);
+  best[1] = best_plan.items ? best_plan.items : 8u;
+  best[2] = log_n <= kMaxT ? 5u : (best_plan.top_radix ? best_plan.top_radix : 3u);
+  return check_cuda(cudaStreamSynchronize(st), "vs_autotune_lde");
 }
 
 }  // extern "C"

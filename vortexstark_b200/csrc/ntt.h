@@ -29,6 +29,7 @@ struct NttPass {
   uint32_t a, b, c;                 // layers [a, b]; c low index bits per tile row
   uint32_t src_mask;
   uint32_t scale;                   // inverse scale applied after the last layer (0: none)
+  uint32_t items;                   // tiles per CTA before it retires (host side; 0: 8)
   NttTw tw;
 };
 
@@ -43,7 +44,18 @@ struct NttColumns {
 
 struct PassRange { uint32_t a, b, c; };
 
-std::vector<PassRange> plan_passes(uint32_t log_n);
+// Launch shape of the transforms of one size, set by the autotuner
+// (vs_autotune_lde) or vs_ntt_plan_set. Zero fields take the defaults. A plan
+// changes how the butterfly layers are grouped into kernels, never the result.
+struct NttPlan {
+  uint32_t lower;      // layers of the first (lower) pass; default 13
+  uint32_t items;      // tiles a pass CTA transforms before retiring; default 8
+  uint32_t top_radix;  // layers per register round of the LDE top pass: 3 (16-byte chunks) or 5 (words); default 3
+};
+NttPlan ntt_plan(uint32_t log_n);
+bool ntt_plan_valid(uint32_t log_n, const NttPlan& p);
+std::vector<NttPlan> ntt_plan_candidates(uint32_t log_n);
+std::vector<PassRange> plan_passes(uint32_t log_n, uint32_t lower = 0);
 uint32_t inv_n_scale(uint32_t log_n);
 NttTw native_tw(const uint32_t* line, const uint32_t* circle, const uint32_t* offsets, uint32_t n_line_layers);
 NttTw stwo_tw(const uint32_t* flat, uint32_t log_n);
