@@ -228,13 +228,14 @@ int vs_lde_native(const uint32_t* d_src, uint64_t src_stride, uint32_t* d_dst, u
  *              max(5, log_n - 11) .. 13, other sizes only their default
  *              (13, or log_n below 14);
  *   items      tiles a pass CTA transforms before it retires, 1..64 (0: 8);
- *   top_radix  layers per register round of the LDE top pass above 13 layers:
- *              3 (16-byte chunks, the default) or 5 (words); 0: default.
+ *   radix      layers per register round above a C = 0 tile's first five:
+ *              3 (16-byte chunk rounds, the default) or 5 (word rounds); 0: default.
+ *              The LDE of at most 13 layers has the word-round form only.
  * Plans change only how layers are grouped into launches; results are identical.
  * vs_ntt_plan_set(log_n, 0, 0, 0) restores the defaults. */
-int vs_ntt_plan_set(uint32_t log_n, uint32_t lower, uint32_t items, uint32_t top_radix);
-int vs_ntt_plan_get(uint32_t log_n, uint32_t* lower, uint32_t* items, uint32_t* top_radix);
-/* The plans the autotuner tries for log_n, 3 words each (lower, items, top_radix);
+int vs_ntt_plan_set(uint32_t log_n, uint32_t lower, uint32_t items, uint32_t radix);
+int vs_ntt_plan_get(uint32_t log_n, uint32_t* lower, uint32_t* items, uint32_t* radix);
+/* The plans the autotuner tries for log_n, 3 words each (lower, items, radix);
  * *n_out = their number (host only, no device calls). */
 int vs_ntt_plan_candidates(uint32_t log_n, uint32_t* out, uint32_t cap, uint32_t* n_out);
 /* Times every candidate plan on an n_cols-column stwo LDE of 2^log_n rows (seeded

@@ -19,7 +19,7 @@ def test_candidates_shape():
         for lower, items, radix in cands:
             assert items in (4, 8, 16)
             if log_n <= 13:
-                assert (lower, radix) == (log_n, 5)
+                assert (lower, radix) == (log_n, 3)
             else:
                 assert radix in (3, 5)
                 assert 10 <= lower <= 13 and log_n - lower <= 11 if log_n <= 24 else lower == 13
@@ -29,7 +29,7 @@ def test_candidates_shape():
 
 def test_set_get_round_trip_and_defaults():
     assert api.ntt_plan(24) == (13, 8, 3)
-    assert api.ntt_plan(12) == (12, 8, 5)
+    assert api.ntt_plan(12) == (12, 8, 3)
     for log_n in (8, 14, 20, 24, 28):
         for plan in api.ntt_plan_candidates(log_n):
             api.set_ntt_plan(log_n, *plan)

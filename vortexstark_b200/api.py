@@ -118,15 +118,15 @@ def init_memory_pool(release_threshold_bytes: int = 2 << 30) -> None:
 
 
 def ntt_plan(log_n: int) -> tuple[int, int, int]:
-    """(lower pass layers, tiles per CTA, LDE top-pass round layers) used for 2^log_n transforms."""
+    """(lower pass layers, tiles per CTA, register-round radix) used for 2^log_n transforms."""
     v = [C.c_uint32() for _ in range(3)]
     check(lib().vs_ntt_plan_get(log_n, *[C.byref(x) for x in v]), "vs_ntt_plan_get")
     return tuple(int(x.value) for x in v)
 
 
-def set_ntt_plan(log_n: int, lower: int = 0, items: int = 0, top_radix: int = 0) -> None:
+def set_ntt_plan(log_n: int, lower: int = 0, items: int = 0, radix: int = 0) -> None:
     """Sets the launch shape of 2^log_n transforms (zeros restore the defaults)."""
-    check(lib().vs_ntt_plan_set(log_n, lower, items, top_radix), "vs_ntt_plan_set")
+    check(lib().vs_ntt_plan_set(log_n, lower, items, radix), "vs_ntt_plan_set")
 
 
 def ntt_plan_candidates(log_n: int) -> list[tuple[int, int, int]]:
@@ -149,7 +149,7 @@ def autotune_lde(log_n: int, n_cols: int = 34, blowup: int = 2, reps: int = 3, s
 
 
 def save_tuning(path, log_ns=range(5, 31)) -> None:
-    """Writes the current plans as JSON ({log_n: [lower, items, top_radix]})."""
+    """Writes the current plans as JSON ({log_n: [lower, items, radix]})."""
     import json
     with open(path, "w") as f:
         json.dump({str(l): list(ntt_plan(l)) for l in log_ns}, f, indent=1)

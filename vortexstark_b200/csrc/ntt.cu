@@ -9,9 +9,11 @@
 //
 // Execution: a transform is split into passes over contiguous layer ranges
 // [a, b]. A pass loads tiles of 2^(b-a+1) x 2^c elements (c low index bits kept
-// for coalescing) into shared memory, runs its layers as register rounds of up
-// to five layers (32 elements per thread, no barrier inside a round) and writes
-// the tile back once. The shared tile uses a 16-byte-chunk XOR swizzle (swz)
+// for coalescing) into shared memory, runs its layers as register rounds (32
+// elements per thread, no barrier inside a round) and writes the tile back once.
+// By default a round above the tile's first five bits holds eight 16-byte chunks
+// along three layers (128-bit shared-memory traffic, one twiddle per chunk);
+// the five-layer word rounds remain as the radix-5 plan the autotuner can pick. The shared tile uses a 16-byte-chunk XOR swizzle (swz)
 // that keeps every round's access pattern bank-conflict free. Pass kernels loop
 // over up to 8 tiles per CTA and double-buffer them: the next tile
 // streams in with 16-byte cp.async copies while the current one is transformed,
@@ -394,12 +396,14 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 2) ntt_lde_top_kernel(NttPas
 // The tile uses swz<0> (chunk index XOR word bits 5-7), which keeps every
 // quarter-warp of these 128-bit accesses on eight distinct chunk positions for
 // every round shape with C >= 2 (round bits at or above word bit 2).
-template <int M, int C>
+// Chunk rounds cover tile bits [S0, C + M): S0 = C for upper tiles, S0 = 5 for
+// C = 0 tiles whose bits 0-4 run first as one five-layer word round.
+template <int M, int C, int S0 = C>
 struct Tile4 {
-  static_assert(C >= 2, "chunk rounds need at least two contiguous index bits");
-  static constexpr int T = M + C, NT = 1 << (T - 5), SIZE = 1 << T, NR = (M + 2) / 3;
-  static constexpr int P0(int r) { return C + 3 * r; }
-  static constexpr int R(int r) { return 3 * (r + 1) <= M ? 3 : M - 3 * r; }
+  static_assert(S0 >= 2 && S0 >= C, "chunk rounds need two contiguous index bits below them");
+  static constexpr int T = M + C, NT = 1 << (T - 5), SIZE = 1 << T, MC = T - S0, NR = (MC + 2) / 3;
+  static constexpr int P0(int r) { return S0 + 3 * r; }
+  static constexpr int R(int r) { return 3 * (r + 1) <= MC ? 3 : MC - 3 * r; }
 };
 
 // Word address of chunk k (R round bits at word bit P0) of chunk group o; o
@@ -413,7 +417,7 @@ __device__ __forceinline__ uint32_t ins4(uint32_t o, uint32_t k) {
 template <int M, int C>
 __device__ __forceinline__ void tile_load4(uint32_t* sm, const uint32_t* __restrict__ src, const TileGeo& g,
                                            uint32_t mask) {
-  using S = Tile4<M, C>;
+  using S = Tile<M, C>;
 #pragma unroll
   for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
     const uint32_t e = 4 * (threadIdx.x + i * S::NT);
@@ -422,7 +426,7 @@ __device__ __forceinline__ void tile_load4(uint32_t* sm, const uint32_t* __restr
 }
 template <int M, int C>
 __device__ __forceinline__ void tile_store4(const uint32_t* sm, uint32_t* __restrict__ dst, const TileGeo& g) {
-  using S = Tile4<M, C>;
+  using S = Tile<M, C>;
 #pragma unroll
   for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
     const uint32_t e = 4 * (threadIdx.x + i * S::NT);
@@ -430,9 +434,9 @@ __device__ __forceinline__ void tile_store4(const uint32_t* sm, uint32_t* __rest
   }
 }
 
-template <int M, int C, int r>
+template <int M, int C, int r, int S0 = C>
 __device__ __forceinline__ void rload4(uint4 (&v)[8], const uint32_t* sm) {
-  using S = Tile4<M, C>;
+  using S = Tile4<M, C, S0>;
   constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (3 - R);
 #pragma unroll
   for (int s = 0; s < SUB; s++)
@@ -440,9 +444,9 @@ __device__ __forceinline__ void rload4(uint4 (&v)[8], const uint32_t* sm) {
     for (int k = 0; k < K; k++)
       v[s * K + k] = *reinterpret_cast<const uint4*>(sm + swz<0>(ins4<P0, R>(threadIdx.x + s * S::NT, k)));
 }
-template <int M, int C, int r>
+template <int M, int C, int r, int S0 = C>
 __device__ __forceinline__ void rstore4(const uint4 (&v)[8], uint32_t* sm) {
-  using S = Tile4<M, C>;
+  using S = Tile4<M, C, S0>;
   constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (3 - R);
 #pragma unroll
   for (int s = 0; s < SUB; s++)
@@ -462,9 +466,9 @@ __device__ __forceinline__ void bfly4(uint4& a, uint4& b, uint32_t tt) {
 // Butterflies of chunk round r; layer q of the round (tile bit p = P0 + q) is
 // global layer a + p - C with group index h = hi * 2^(T-1-p) + (address >> (p+1)).
 // Twiddle tables are 16-byte aligned up to their size (host-checked), as for rbfly.
-template <bool FWD, int M, int C, int r>
+template <bool FWD, int M, int C, int r, int S0 = C>
 __device__ __forceinline__ void rbfly4(uint4 (&v)[8], const TileGeo& g, const NttTw& tw) {
-  using S = Tile4<M, C>;
+  using S = Tile4<M, C, S0>;
   constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (3 - R), T = S::T;
 #pragma unroll
   for (int s = 0; s < SUB; s++) {
@@ -506,12 +510,21 @@ __device__ __forceinline__ void rbfly4(uint4 (&v)[8], const TileGeo& g, const Nt
   }
 }
 
-template <bool FWD, int M, int C, int r>
-__device__ __forceinline__ void round4(uint32_t* sm, const TileGeo& g, const NttTw& tw) {
+template <bool FWD, int M, int C, int r, int S0 = C>
+__device__ __forceinline__ void round4(uint32_t* sm, const TileGeo& g, const NttTw& tw, uint32_t scale = 0) {
   uint4 v[8];
-  rload4<M, C, r>(v, sm);
-  rbfly4<FWD, M, C, r>(v, g, tw);
-  rstore4<M, C, r>(v, sm);
+  rload4<M, C, r, S0>(v, sm);
+  rbfly4<FWD, M, C, r, S0>(v, g, tw);
+  if (scale) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      v[k].x = mul(v[k].x, scale);
+      v[k].y = mul(v[k].y, scale);
+      v[k].z = mul(v[k].z, scale);
+      v[k].w = mul(v[k].w, scale);
+    }
+  }
+  rstore4<M, C, r, S0>(v, sm);
 }
 // Rounds [lo, hi] in transform order (forward: hi down to lo), barrier after each.
 template <bool FWD, int M, int C>
@@ -576,12 +589,87 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPa
   }
 }
 
+// Chunk-round form of the pass kernel (same persistent, double-buffered
+// structure as ntt_pass_kernel). C = 0 tiles run tile bits 0-4 as one five-layer
+// word round and the layers above as three-layer chunk rounds; upper tiles
+// (C >= 2) run chunk rounds only. Both use the swz<0> tile layout.
+template <int M, int C>
+__device__ __forceinline__ void tile_load_async4(uint32_t* sm, const uint32_t* __restrict__ src, const TileGeo& g,
+                                                 uint32_t mask) {
+  using S = Tile<M, C>;
+  const uint32_t base = smem_addr(sm);
+#pragma unroll
+  for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
+    const uint32_t e = 4 * (threadIdx.x + i * S::NT);
+    cp_async16(base + 4 * swz<0>(e), src + (gidx<M, C>(g, e) & mask));
+  }
+}
+template <bool FWD, int M, int C, int S0>
+__device__ __forceinline__ void chunk_round(int r, uint32_t* sm, const TileGeo& g, const NttTw& tw, uint32_t scale) {
+  using S4 = Tile4<M, C, S0>;
+  switch (r) {
+    case 0: round4<FWD, M, C, 0, S0>(sm, g, tw, scale); break;
+    case 1: round4<FWD, M, C, (S4::NR > 1 ? 1 : 0), S0>(sm, g, tw, scale); break;
+    case 2: round4<FWD, M, C, (S4::NR > 2 ? 2 : 0), S0>(sm, g, tw, scale); break;
+    default: round4<FWD, M, C, (S4::NR > 3 ? 3 : 0), S0>(sm, g, tw, scale); break;
+  }
+}
+template <bool FWD, int M, int C>
+__global__ void __launch_bounds__(1 << (M + C - 5), (M + C == 13) ? 3 : 2) ntt_pass4_kernel(NttPass p, uint32_t n_cols,
+                                                                     uint32_t total) {
+  constexpr int S0 = C == 0 ? 5 : C;
+  using S4 = Tile4<M, C, S0>;
+  static_assert(S4::NR >= 1 && S4::NR <= 4, "one to four chunk rounds");
+  constexpr int SIZE = 1 << (M + C);
+  extern __shared__ __align__(16) uint32_t pass4_sm[];
+  uint32_t w = blockIdx.x;
+  if (w >= total) return;
+  tile_load_async4<M, C>(pass4_sm, col_src(p, w % n_cols), tile_geo<M, C>(p.a, w / n_cols), p.src_mask);
+  cp_async_commit();
+  for (uint32_t it = 0; w < total; it++, w += gridDim.x) {
+    uint32_t* sm = pass4_sm + (it & 1) * SIZE;
+    const uint32_t nw = w + gridDim.x;
+    if (nw < total)
+      tile_load_async4<M, C>(pass4_sm + ((it + 1) & 1) * SIZE, col_src(p, nw % n_cols),
+                             tile_geo<M, C>(p.a, nw / n_cols), p.src_mask);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    const TileGeo g = tile_geo<M, C>(p.a, w / n_cols);
+    if (!FWD) {
+      if (C == 0) {
+        round_sm<false, M, C, 0>(sm, g, p.tw, 0);
+        __syncthreads();
+      }
+#pragma unroll
+      for (int r = 0; r < S4::NR; r++) {
+        chunk_round<false, M, C, S0>(r, sm, g, p.tw, r == S4::NR - 1 ? p.scale : 0u);
+        __syncthreads();
+      }
+    } else {
+#pragma unroll
+      for (int r = S4::NR - 1; r >= 0; r--) {
+        chunk_round<true, M, C, S0>(r, sm, g, p.tw, 0u);
+        __syncthreads();
+      }
+      if (C == 0) {
+        round_sm<true, M, C, 0>(sm, g, p.tw, 0);
+        __syncthreads();
+      }
+    }
+    tile_store4<M, C>(sm, col_dst(p, w % n_cols), g);
+    __syncthreads();  // this buffer is refilled by the next iteration's prefetch
+  }
+}
+
 // Launch tables: single / lower passes use C = 0 (T = M, 5 <= M <= 13); upper
 // passes use T = 13 (C = 13 - M, 1 <= M <= 11).
 using PassFn = void (*)(NttPass, uint32_t, uint32_t);
 using TopFn = void (*)(NttPass, NttPass, uint32_t);
 template <bool FWD, int M> PassFn pass_lo() { return ntt_pass_kernel<FWD, M, 0>; }
 template <bool FWD, int M> PassFn pass_hi() { return ntt_pass_kernel<FWD, M, 13 - M>; }
+template <bool FWD, int M> PassFn pass4_lo() { return ntt_pass4_kernel<FWD, M, 0>; }
+template <bool FWD, int M> PassFn pass4_hi() { return ntt_pass4_kernel<FWD, M, 13 - M>; }
 template <int M> TopFn top_lo() { return ntt_lde_top_kernel<M, 0>; }
 template <int M> TopFn top_hi() { return ntt_lde_top4_kernel<M, 13 - M>; }
 template <int M> TopFn top5_hi() { return ntt_lde_top_kernel<M, 13 - M>; }
@@ -592,6 +680,19 @@ static PassFn pass_fn(bool fwd, uint32_t M, uint32_t C) {
   if (C == 0) {
     switch (M) { VS_LO(5) VS_LO(6) VS_LO(7) VS_LO(8) VS_LO(9) VS_LO(10) VS_LO(11) VS_LO(12) VS_LO(13) default: break; }
   } else if (M + C == 13) {
+    switch (M) { VS_HI(1) VS_HI(2) VS_HI(3) VS_HI(4) VS_HI(5) VS_HI(6) VS_HI(7) VS_HI(8) VS_HI(9) VS_HI(10) VS_HI(11) default: break; }
+  }
+#undef VS_LO
+#undef VS_HI
+  return nullptr;
+}
+// Chunk-round passes: C = 0 with more than five layers, or upper tiles.
+static PassFn pass4_fn(bool fwd, uint32_t M, uint32_t C) {
+#define VS_LO(m) case m: return fwd ? pass4_lo<true, m>() : pass4_lo<false, m>();
+#define VS_HI(m) case m: return fwd ? pass4_hi<true, m>() : pass4_hi<false, m>();
+  if (C == 0) {
+    switch (M) { VS_LO(6) VS_LO(7) VS_LO(8) VS_LO(9) VS_LO(10) VS_LO(11) VS_LO(12) VS_LO(13) default: break; }
+  } else if (M + C == 13 && C >= 2) {
     switch (M) { VS_HI(1) VS_HI(2) VS_HI(3) VS_HI(4) VS_HI(5) VS_HI(6) VS_HI(7) VS_HI(8) VS_HI(9) VS_HI(10) VS_HI(11) default: break; }
   }
 #undef VS_LO
@@ -658,7 +759,7 @@ static bool lower_valid(uint32_t L, uint32_t lower) {
   return lower >= std::max<uint32_t>(5, L - (kMaxT - kMinC)) && lower <= kMaxT;
 }
 bool ntt_plan_valid(uint32_t L, const NttPlan& p) {
-  return L < 32 && lower_valid(L, p.lower) && p.items <= 64 && (p.top_radix == 0 || p.top_radix == 3 || p.top_radix == 5);
+  return L < 32 && lower_valid(L, p.lower) && p.items <= 64 && (p.radix == 0 || p.radix == 3 || p.radix == 5);
 }
 NttPlan ntt_plan(uint32_t L) {
   NttPlan p{};
@@ -667,7 +768,7 @@ NttPlan ntt_plan(uint32_t L) {
     p = g_plan[L];
   }
   if (!p.items) p.items = 8;
-  if (!p.top_radix) p.top_radix = 3;
+  if (!p.radix) p.radix = 3;
   return p;
 }
 static void set_plan(uint32_t L, const NttPlan& p) {
@@ -746,7 +847,8 @@ static uint32_t persistent_grid(const void* fn, uint32_t threads, uint32_t smem)
 
 static int launch_pass(NttPass p, bool fwd, uint32_t n_cols, cudaStream_t st) {
   const uint32_t M = p.b - p.a + 1, T = M + p.c;
-  PassFn fn = pass_fn(fwd, M, p.c);
+  PassFn fn = p.radix == 5 ? nullptr : pass4_fn(fwd, M, p.c);
+  if (!fn) fn = pass_fn(fwd, M, p.c);
   if (!fn) return set_error(VS_ERR_INVALID, "ntt: no kernel for pass shape M=%u C=%u", M, p.c);
   const uint32_t tile_bits = p.log_n - T;
   const uint64_t total = (uint64_t)n_cols << tile_bits;
@@ -901,6 +1003,7 @@ static int ntt_transform_aligned(const NttColumns& io, uint32_t L, const NttTw& 
     NttPass p{};
     p.tw = tw;
     p.items = plan.items;
+    p.radix = plan.radix;
     p.log_n = L;
     p.a = r.a;
     p.b = r.b;
@@ -954,6 +1057,7 @@ static int ntt_lde_aligned(const NttColumns& io, uint32_t l, uint32_t B, const N
     NttPass p{};
     p.tw = tw_inv;
     p.items = plan.items;
+    p.radix = plan.radix;
     p.log_n = l;
     p.a = passes[i].a;
     p.b = passes[i].b;
@@ -984,7 +1088,7 @@ static int ntt_lde_aligned(const NttColumns& io, uint32_t l, uint32_t B, const N
     pf.dst = io.dst;
     pf.dst_stride = io.dst_stride;
     const uint32_t M = r.b - r.a + 1, T = M + r.c;
-    TopFn fn = top_fn(M, r.c, plan.top_radix);
+    TopFn fn = top_fn(M, r.c, plan.radix);
     if (!fn) return set_error(VS_ERR_INVALID, "ntt: no LDE kernel for shape M=%u C=%u", M, r.c);
     const uint32_t smem = 8u << T;  // working tile + coefficient tile
     VS_TRY(allow_smem((const void*)fn, smem));
@@ -996,6 +1100,7 @@ static int ntt_lde_aligned(const NttColumns& io, uint32_t l, uint32_t B, const N
     NttPass p{};
     p.tw = tw_fwd;
     p.items = plan.items;
+    p.radix = plan.radix;
     p.log_n = l + B;
     p.a = passes[i].a;
     p.b = passes[i].b;
@@ -1222,26 +1327,25 @@ int vs_lde_native(const uint32_t* src, uint64_t src_stride, uint32_t* dst, uint6
 }
 
 // ------------------------------------------------------------------ autotuner
-int vs_ntt_plan_set(uint32_t log_n, uint32_t lower, uint32_t items, uint32_t top_radix) {
+int vs_ntt_plan_set(uint32_t log_n, uint32_t lower, uint32_t items, uint32_t radix) {
   clear_error();
-  // canonical form: the default lower pass (13, or the whole transform up to 13
-  // layers) is 0, and below 14 layers the top pass has only the five-layer form
+  // canonical form: the default lower pass (13, or the whole transform up to 13 layers) is 0
   const uint32_t lo = (lower == kMaxT || (log_n <= kMaxT && lower == log_n)) ? 0u : lower;
-  const uint32_t rx = (log_n <= kMaxT && top_radix == 5) ? 0u : top_radix;
+  const uint32_t rx = radix;
   const NttPlan p{lo, items, rx};
   if (!ntt_plan_valid(log_n, p))
     return set_error(VS_ERR_INVALID, "vs_ntt_plan_set: no plan (lower %u, items %u, radix %u) for log_n %u", lower,
-                     items, top_radix, log_n);
+                     items, radix, log_n);
   set_plan(log_n, p);
   return VS_OK;
 }
-int vs_ntt_plan_get(uint32_t log_n, uint32_t* lower, uint32_t* items, uint32_t* top_radix) {
+int vs_ntt_plan_get(uint32_t log_n, uint32_t* lower, uint32_t* items, uint32_t* radix) {
   clear_error();
-  if (log_n >= 32 || !lower || !items || !top_radix) return set_error(VS_ERR_INVALID, "vs_ntt_plan_get: bad argument");
+  if (log_n >= 32 || !lower || !items || !radix) return set_error(VS_ERR_INVALID, "vs_ntt_plan_get: bad argument");
   const NttPlan p = ntt_plan(log_n);
   *lower = log_n <= kMaxT ? log_n : (p.lower ? p.lower : kMaxT);
   *items = p.items;
-  *top_radix = log_n <= kMaxT ? 5u : p.top_radix;
+  *radix = p.radix;
   return VS_OK;
 }
 int vs_ntt_plan_candidates(uint32_t log_n, uint32_t* out, uint32_t cap, uint32_t* n_out) {
@@ -1252,7 +1356,7 @@ int vs_ntt_plan_candidates(uint32_t log_n, uint32_t* out, uint32_t cap, uint32_t
   for (uint32_t i = 0; i < v.size() && i < cap && out; i++) {
     out[3 * i] = v[i].lower ? v[i].lower : std::min<uint32_t>(log_n, kMaxT);
     out[3 * i + 1] = v[i].items;
-    out[3 * i + 2] = v[i].top_radix ? v[i].top_radix : 5u;
+    out[3 * i + 2] = v[i].radix ? v[i].radix : 3u;
   }
   return VS_OK;
 }
@@ -1308,7 +1412,7 @@ int vs_autotune_lde(uint32_t log_n, uint32_t n_cols, uint32_t blowup_bits, uint3
   if (rc != VS_OK) return rc;
   best[0] = best_plan.lower ? best_plan.lower : std::min<uint32_t>(log_n, kMaxT);
   best[1] = best_plan.items ? best_plan.items : 8u;
-  best[2] = log_n <= kMaxT ? 5u : (best_plan.top_radix ? best_plan.top_radix : 3u);
+  best[2] = best_plan.radix ? best_plan.radix : 3u;
   return check_cuda(cudaStreamSynchronize(st), "vs_autotune_lde");
 }
 

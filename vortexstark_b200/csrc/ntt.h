@@ -30,6 +30,7 @@ struct NttPass {
   uint32_t src_mask;
   uint32_t scale;                   // inverse scale applied after the last layer (0: none)
   uint32_t items;                   // tiles per CTA before it retires (host side; 0: 8)
+  uint32_t radix;                   // 3: chunk-round kernels, 5: word-round kernels (host side; 0: 3)
   NttTw tw;
 };
 
@@ -50,7 +51,7 @@ struct PassRange { uint32_t a, b, c; };
 struct NttPlan {
   uint32_t lower;      // layers of the first (lower) pass; default 13
   uint32_t items;      // tiles a pass CTA transforms before retiring; default 8
-  uint32_t top_radix;  // layers per register round of the LDE top pass: 3 (16-byte chunks) or 5 (words); default 3
+  uint32_t radix;      // layers per register round above the first five: 3 (16-byte chunks) or 5 (words); default 3
 };
 NttPlan ntt_plan(uint32_t log_n);
 bool ntt_plan_valid(uint32_t log_n, const NttPlan& p);
