@@ -500,6 +500,10 @@ def main():
             tuning[str(tl)] = {"plan": list(r["best"]), "ms": times[tuple(r["best"])],
                                "default_plan": list(default), "default_ms": times.get(tuple(default)),
                                "candidates": len(times)}
+        # Merkle subtree split of the root-only trees, tuned on the step's row-packed root
+        m = api.autotune_merkle(args.log_n + 2, n_cols=args.cols, reps=3)
+        tuning["merkle_split"] = {"split": m["best"], "ms_by_split": [round(x, 3) for x in m["ms"]],
+                                  "log_leaves": args.log_n + 2}
 
     n_cols, log_n, blow, fri_log, N, committed = workload(args)
     n = 1 << log_n

@@ -244,6 +244,21 @@ int vs_ntt_plan_candidates(uint32_t log_n, uint32_t* out, uint32_t cap, uint32_t
  * candidate i's time per LDE. Allocates its scratch columns on `stream`. */
 int vs_autotune_lde(uint32_t log_n, uint32_t n_cols, uint32_t blowup_bits, uint32_t reps, uint32_t* best,
                     float* ms, uint32_t cap, vs_stream_t stream);
+/* Merkle subtree shape of the root-only trees (no counterpart in the reference):
+ * the first reduction level stops at 2^split roots per 1024-leaf tile (0..8), so a
+ * CTA skips the narrow top levels of its tile, and the next level reduces them.
+ * Roots are identical for every split. Process wide; applies to vs_commit_columns,
+ * vs_merkle_root_rowpacked / _capped / _soa4, vs_fri_fold_commit, the Cairo FRI and
+ * the engine's commitment jobs (their scratch is sized for split 8). */
+int vs_merkle_split_set(uint32_t split);
+uint32_t vs_merkle_split_get(void);
+/* Times the row-packed root of n_cols seeded columns x 2^log_leaves rows (11..28) at
+ * every split (one warm-up and `reps` timed runs each, CUDA events on `stream`),
+ * checks that all splits give one root, keeps the fastest split and writes it to
+ * *best; ms[s] (s < cap) receives split s's time per root. Allocates its scratch on
+ * `stream`. */
+int vs_autotune_merkle(uint32_t log_leaves, uint32_t n_cols, uint32_t reps, uint32_t* best, float* ms, uint32_t cap,
+                       vs_stream_t stream);
 
 /* Merkle root over n_cols columns of 2^log_leaves rows with the row-packed
  * multi-block leaf (all columns, merkle_leaves_lifted.cu semantics with equal

@@ -43,3 +43,20 @@ def test_set_get_round_trip_and_defaults():
 def test_invalid_plans_rejected(log_n, plan):
     with pytest.raises(VstarkError):
         api.set_ntt_plan(log_n, *plan)
+
+
+def test_merkle_split_set_get_and_tuning_file(tmp_path):
+    assert api.merkle_split() == 0
+    for s in range(9):
+        api.set_merkle_split(s)
+        assert api.merkle_split() == s
+    with pytest.raises(VstarkError):
+        api.set_merkle_split(9)
+    api.set_ntt_plan(20, 11, 4, 5)
+    path = tmp_path / "tuning.json"
+    api.save_tuning(path)
+    api.set_merkle_split(0)
+    api.set_ntt_plan(20)
+    api.load_tuning(path)
+    assert api.merkle_split() == 8 and api.ntt_plan(20) == (11, 4, 5)
+    api.set_merkle_split(0)

@@ -84,3 +84,46 @@ def test_autotune_keeps_a_candidate_and_results(L):
     rng = np.random.default_rng(9)
     cols = rand_m31(rng, 2, 1 << log_n)
     assert np.array_equal(_lde(L, cols, log_n), O.stwo_lde_columns(cols, log_n, 2, threads=4))
+
+
+# ------------------------------------------------------------------ Merkle split
+@pytest.fixture
+def default_split():
+    yield
+    if torch.cuda.is_available():
+        api.set_merkle_split(0)
+
+
+@pytest.mark.parametrize("log_n,n_cols", [(11, 34), (15, 34), (17, 5)])
+def test_every_split_gives_the_oracle_roots(L, default_split, log_n, n_cols):
+    from gpu_util import u32_host
+    rng = np.random.default_rng(900 + log_n)
+    cols = rand_m31(rng, n_cols, 1 << log_n)
+    exp_rp = O.merkle_root_rowpacked(cols, threads=4)
+    n_cap = min(16, n_cols)
+    exp_cap = O.merkle_root_capped(cols[:n_cap], threads=4)
+    fri_log = log_n
+    src = rand_m31(rng, 4, 1 << fri_log)
+    alphas = rand_m31(rng, fri_log - 3, 4)
+    er = np.zeros((fri_log - 3, 8), np.uint32)
+    el = np.zeros((8, 4), np.uint32)
+    O.lib().oracle_bench_fri(O.ptr_array(list(src)), fri_log, O.ptr(alphas.reshape(-1).copy()), 4, O.ptr(er), O.ptr(el))
+    d_cols = dev(cols.reshape(-1))
+    for split in range(9):
+        api.set_merkle_split(split)
+        root = empty(8)
+        V.check(L.vs_merkle_root_rowpacked(ptr(d_cols), 1 << log_n, n_cols, log_n, ptr(root), None), "rowpacked")
+        assert np.array_equal(host(root), exp_rp), split
+        V.check(L.vs_merkle_root_capped(ptr(d_cols), 1 << log_n, n_cap, log_n, ptr(root), None), "capped")
+        assert np.array_equal(host(root), exp_cap), split
+        work, roots, last = empty(4 << fri_log), empty(8 * (fri_log - 3)), empty(32)
+        V.check(L.vs_fri_fold_commit(ptr(dev(src.reshape(-1))), fri_log, u32_host(alphas.reshape(-1)), ptr(work),
+                                     ptr(roots), ptr(last), None), "vs_fri_fold_commit")
+        assert np.array_equal(host(roots).reshape(-1, 8), er), split
+        assert np.array_equal(host(last).reshape(8, 4), el), split
+
+
+def test_autotune_merkle_keeps_a_split(L, default_split):
+    res = api.autotune_merkle(16, n_cols=34, reps=2)
+    assert 0 <= res["best"] <= 8 and api.merkle_split() == res["best"]
+    assert all(t > 0 for t in res["ms"]) and res["ms"][res["best"]] == min(res["ms"])

@@ -148,18 +148,39 @@ def autotune_lde(log_n: int, n_cols: int = 34, blowup: int = 2, reps: int = 3, s
     return {"best": tuple(best), "candidates": [(c, float(ms[i])) for i, c in enumerate(cands)]}
 
 
+def merkle_split() -> int:
+    """First-level split of root-only Merkle trees (2^split roots per 1024-leaf tile)."""
+    return int(lib().vs_merkle_split_get())
+
+
+def set_merkle_split(split: int) -> None:
+    check(lib().vs_merkle_split_set(split), "vs_merkle_split_set")
+
+
+def autotune_merkle(log_leaves: int, n_cols: int = 34, reps: int = 3, stream=None) -> dict:
+    """Times the row-packed root at every split, keeps the fastest; {"best": s, "ms": [...]}."""
+    best = C.c_uint32()
+    ms = (C.c_float * 9)()
+    check(lib().vs_autotune_merkle(log_leaves, n_cols, reps, C.byref(best), ms, 9, _stream(stream)),
+          "vs_autotune_merkle")
+    return {"best": int(best.value), "ms": [float(x) for x in ms]}
+
+
 def save_tuning(path, log_ns=range(5, 31)) -> None:
-    """Writes the current plans as JSON ({log_n: [lower, items, radix]})."""
+    """Writes the current NTT plans ({log_n: [lower, items, radix]}) and Merkle split as JSON."""
     import json
     with open(path, "w") as f:
-        json.dump({str(l): list(ntt_plan(l)) for l in log_ns}, f, indent=1)
+        json.dump({"ntt": {str(l): list(ntt_plan(l)) for l in log_ns}, "merkle_split": merkle_split()}, f, indent=1)
 
 
 def load_tuning(path) -> None:
     import json
     with open(path) as f:
-        for k, v in json.load(f).items():
-            set_ntt_plan(int(k), *v)
+        t = json.load(f)
+    for k, v in t.get("ntt", {}).items():
+        set_ntt_plan(int(k), *v)
+    if "merkle_split" in t:
+        set_merkle_split(int(t["merkle_split"]))
 
 
 def launch_count() -> int:

@@ -909,7 +909,8 @@ extern "C" int vs_cairo_oods_fri(void* channel, vs_cairo_oods_fri_io* io, vs_str
   // (prover.rs:2321-2381)
   uint32_t *fri = nullptr, *mscratch = nullptr;
   VS_TRY(s.alloc(&fri, 4 * N));
-  VS_TRY(s.alloc(&mscratch, merkle_scratch_words(N / 2)));
+  VS_TRY(s.alloc(&mscratch, merkle_scratch_words(N / 2, MK_MAX_SPLIT)));
+  const uint32_t split = merkle_split();
   uint32_t* src[4] = {oq[0], oq[1], oq[2], oq[3]};
   uint32_t* dst[4];
   uint64_t off = 0;
@@ -921,7 +922,7 @@ extern "C" int vs_cairo_oods_fri(void* channel, vs_cairo_oods_fri_io* io, vs_str
   uint64_t half = N / 2;
   for (int k = 0; k < 4; k++) dst[k] = fri + off + k * half;
   off += 4 * half;
-  VS_TRY(fold_commit_layer(src, dst, tw, fa.v, nullptr, false, half, d_root, mscratch, st));
+  VS_TRY(fold_commit_layer(src, dst, tw, fa.v, nullptr, false, half, d_root, mscratch, st, split));
   for (uint32_t cur = log_eval - 1; cur > 3; cur--) {
     VS_TRY(read_hash(d_root, root, st));
     ch->mix_digest(root);
@@ -933,7 +934,7 @@ extern "C" int vs_cairo_oods_fri(void* channel, vs_cairo_oods_fri_io* io, vs_str
     half >>= 1;
     for (int k = 0; k < 4; k++) dst[k] = fri + off + k * half;
     off += 4 * half;
-    VS_TRY(fold_commit_layer(src, dst, tw, fa.v, nullptr, false, half, d_root, mscratch, st));
+    VS_TRY(fold_commit_layer(src, dst, tw, fa.v, nullptr, false, half, d_root, mscratch, st, split));
   }
   std::vector<uint32_t> planes(32);
   for (int k = 0; k < 4; k++)

@@ -71,7 +71,7 @@ int vs_commit_columns(const uint32_t* d_cols, uint32_t n_cols, uint32_t log_n, u
   if (!d_cols || !d_lde || !d_root || !n_cols) return set_error(VS_ERR_INVALID, "vs_commit_columns: bad args");
   const uint64_t n = 1ull << log_n, N = n << blowup;
   VS_TRY(lde_cached(TW_STWO, d_cols, n, d_lde, N, n_cols, log_n, blowup, st));
-  return merkle_root(LeafRowPacked{d_lde, N, n_cols}, N, d_root, st);
+  return merkle_root(LeafRowPacked{d_lde, N, n_cols}, N, d_root, st, nullptr, merkle_split());
 }
 
 }  // extern "C"

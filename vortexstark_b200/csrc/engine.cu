@@ -49,7 +49,7 @@ struct CommitWs {
 
 uint64_t commit_bytes(uint32_t log_n, uint32_t n_cols) {
   const uint64_t n = 1ull << log_n, N = n << 2;
-  return (uint64_t)n_cols * (n + N) * 4 + merkle_scratch_words(N) * 4 + 64;
+  return (uint64_t)n_cols * (n + N) * 4 + merkle_scratch_words(N, MK_MAX_SPLIT) * 4 + 64;
 }
 
 // Jobs run at one of three stream priorities by working-set size (small jobs
@@ -123,7 +123,7 @@ struct Engine {
       VS_CUDA(cudaMalloc(&w->cols, (uint64_t)w->capacity * n * 4));
       VS_CUDA(cudaMalloc(&w->lde, (uint64_t)w->capacity * N * 4));
       VS_CUDA(cudaMalloc(&w->root, 32));
-      VS_CUDA(cudaMalloc(&w->scratch, std::max<uint64_t>(merkle_scratch_words(N), 8) * 4));
+      VS_CUDA(cudaMalloc(&w->scratch, std::max<uint64_t>(merkle_scratch_words(N, MK_MAX_SPLIT), 8) * 4));
       VS_CUDA(cudaMallocHost(&w->h_root, 32));
       w->bytes = commit_bytes(j.log_n, w->capacity);
       const TwiddleSet* t = nullptr;
@@ -157,7 +157,7 @@ struct Engine {
     cudaStream_t st = s.st[level_of(commit_bytes(j.log_n, j.n_cols))];
     VS_TRY(vs_fill_uniform_m31(w->cols, (uint64_t)j.n_cols * n, j.seed, 0, (vs_stream_t)st));
     VS_TRY(lde_cached(TW_STWO, w->cols, n, w->lde, N, j.n_cols, j.log_n, 2, st));
-    VS_TRY(merkle_root(LeafRowPacked{w->lde, N, j.n_cols}, N, w->root, st, w->scratch));
+    VS_TRY(merkle_root(LeafRowPacked{w->lde, N, j.n_cols}, N, w->root, st, w->scratch, merkle_split()));
     VS_CUDA(cudaMemcpyAsync(w->h_root, w->root, 32, cudaMemcpyDeviceToHost, st));
     VS_CUDA(cudaStreamSynchronize(st));
     out.assign((uint8_t*)w->h_root, (uint8_t*)w->h_root + 32);

@@ -37,13 +37,13 @@ __global__ void fold_circle_kernel(Soa4Out dst, Soa4Ptrs src, const uint32_t* __
 // = output size (power of two); twiddles of length half_n.
 int fold_commit_layer(const uint32_t* const src[4], uint32_t* const dst[4], const uint32_t* tw, const uint32_t* alpha,
                       const uint32_t* alpha_sq, bool circle_accumulate, uint64_t half_n, uint32_t* d_root,
-                      uint32_t* scratch, cudaStream_t st) {
+                      uint32_t* scratch, cudaStream_t st, uint32_t split) {
   LeafFold leaf{};
   for (int k = 0; k < 4; k++) { leaf.src.c[k] = src[k]; leaf.dst.c[k] = dst[k]; }
   leaf.tw = tw;
   for (int k = 0; k < 4; k++) { leaf.alpha.v[k] = alpha[k]; leaf.alpha_sq.v[k] = alpha_sq ? alpha_sq[k] : 0; }
   leaf.accumulate = circle_accumulate ? 1 : 0;
-  return merkle_root(leaf, half_n, d_root, st, scratch);
+  return merkle_root(leaf, half_n, d_root, st, scratch, split);
 }
 
 }  // namespace vs
@@ -80,7 +80,8 @@ int vs_fri_fold_commit(const uint32_t* d_src, uint32_t log_n, const uint32_t* h_
   if (log_n < 4 || log_n > 30) return set_error(VS_ERR_INVALID, "vs_fri_fold_commit: log_n %u out of range", log_n);
   const uint64_t N = 1ull << log_n;
   uint32_t* scratch = nullptr;
-  VS_CUDA(cudaMallocAsync((void**)&scratch, (merkle_scratch_words(N / 2) + 8) * 4, st));
+  VS_CUDA(cudaMallocAsync((void**)&scratch, (merkle_scratch_words(N / 2, MK_MAX_SPLIT) + 8) * 4, st));
+  const uint32_t split = merkle_split();
   const uint32_t* src[4] = {d_src, d_src + N, d_src + 2 * N, d_src + 3 * N};
   uint32_t* bufs[2] = {d_work, d_work + 2 * N};  // each holds 4 planes of <= N/2 words
   int rc = VS_OK;
@@ -92,7 +93,8 @@ int vs_fri_fold_commit(const uint32_t* d_src, uint32_t log_n, const uint32_t* h_
     const uint32_t* tw = nullptr;
     rc = get_fold_twiddles(layer == 0 ? COSET_HALF_COSET : COSET_HALF_ODDS, cl, &tw, st);
     if (rc != VS_OK) break;
-    rc = fold_commit_layer(src, dst, tw, h_alphas + 4 * layer, nullptr, false, half, d_roots + 8 * layer, scratch, st);
+    rc = fold_commit_layer(src, dst, tw, h_alphas + 4 * layer, nullptr, false, half, d_roots + 8 * layer, scratch, st,
+                           split);
     for (int k = 0; k < 4; k++) src[k] = dst[k];
     cl--;
   }

@@ -12,6 +12,6 @@ namespace vs {
 // passes circle_accumulate = false.
 int fold_commit_layer(const uint32_t* const src[4], uint32_t* const dst[4], const uint32_t* tw, const uint32_t* alpha,
                       const uint32_t* alpha_sq, bool circle_accumulate, uint64_t half_n, uint32_t* d_root,
-                      uint32_t* scratch, cudaStream_t st);
+                      uint32_t* scratch, cudaStream_t st, uint32_t split = 0);
 
 }  // namespace vs

@@ -1,10 +1,18 @@
 // Blake2s Merkle commitment: drop-in entry points for cuda/blake2s.cu and
 // cuda/merkle_leaves_lifted.cu, and vs_merkle_root_* (root-only commitments).
+#include <atomic>
+#include <cstring>
+
 #include "merkle.h"
 #include "vs_field.cuh"
 #include "vs_mem.cuh"
 
 namespace vs {
+
+// Split of the root-only trees: the first reduction level stops at 2^split roots
+// per 1024-leaf tile (merkle_root). Set by vs_merkle_split_set / vs_autotune_merkle.
+static std::atomic<uint32_t> g_merkle_split{0};
+uint32_t merkle_split() { return g_merkle_split.load(std::memory_order_relaxed); }
 
 template <class Leaf>
 __global__ void leaf_hash_kernel(Leaf leaf, uint64_t n, uint32_t* __restrict__ out) {
@@ -138,19 +146,83 @@ int vs_merkle_root_rowpacked(const uint32_t* d_cols, uint64_t stride, uint32_t n
                              uint32_t* d_root, vs_stream_t st) {
   clear_error();
   if (!d_cols || !d_root || log_leaves > 31) return set_error(VS_ERR_INVALID, "vs_merkle_root_rowpacked: bad args");
-  return merkle_root(LeafRowPacked{d_cols, stride, n_cols}, 1ull << log_leaves, d_root, (cudaStream_t)st);
+  return merkle_root(LeafRowPacked{d_cols, stride, n_cols}, 1ull << log_leaves, d_root, (cudaStream_t)st, nullptr,
+                     merkle_split());
 }
 int vs_merkle_root_capped(const uint32_t* d_cols, uint64_t stride, uint32_t n_cols, uint32_t log_leaves,
                           uint32_t* d_root, vs_stream_t st) {
   clear_error();
   if (!d_cols || !d_root || log_leaves > 31) return set_error(VS_ERR_INVALID, "vs_merkle_root_capped: bad args");
-  return merkle_root(LeafCapped{nullptr, d_cols, stride, n_cols}, 1ull << log_leaves, d_root, (cudaStream_t)st);
+  return merkle_root(LeafCapped{nullptr, d_cols, stride, n_cols}, 1ull << log_leaves, d_root, (cudaStream_t)st, nullptr,
+                     merkle_split());
 }
 int vs_merkle_root_soa4(const uint32_t* c0, const uint32_t* c1, const uint32_t* c2, const uint32_t* c3,
                         uint32_t log_leaves, uint32_t* d_root, vs_stream_t st) {
   clear_error();
   if (!c0 || !c1 || !c2 || !c3 || !d_root || log_leaves > 31) return set_error(VS_ERR_INVALID, "vs_merkle_root_soa4: bad args");
-  return merkle_root(LeafSoa4{c0, c1, c2, c3}, 1ull << log_leaves, d_root, (cudaStream_t)st);
+  return merkle_root(LeafSoa4{c0, c1, c2, c3}, 1ull << log_leaves, d_root, (cudaStream_t)st, nullptr, merkle_split());
+}
+
+int vs_merkle_split_set(uint32_t split) {
+  clear_error();
+  if (split > MK_MAX_SPLIT) return set_error(VS_ERR_INVALID, "vs_merkle_split_set: split %u above %u", split, MK_MAX_SPLIT);
+  g_merkle_split.store(split);
+  return VS_OK;
+}
+uint32_t vs_merkle_split_get(void) { return merkle_split(); }
+
+// Times the row-packed root of n_cols seeded columns of 2^log_leaves rows at every
+// split (one warm-up and `reps` timed runs each, CUDA events on the stream), checks
+// that every split gives the same root, and keeps the fastest split.
+int vs_autotune_merkle(uint32_t log_leaves, uint32_t n_cols, uint32_t reps, uint32_t* best, float* ms_out, uint32_t cap,
+                       vs_stream_t stream) {
+  clear_error();
+  cudaStream_t st = (cudaStream_t)stream;
+  if (log_leaves < 11 || log_leaves > 28 || !n_cols || !best)
+    return set_error(VS_ERR_INVALID, "vs_autotune_merkle: bad size (log %u, cols %u)", log_leaves, n_cols);
+  if (!reps) reps = 3;
+  const uint64_t n = 1ull << log_leaves;
+  uint32_t *cols = nullptr, *scratch = nullptr, *roots = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = check_cuda(cudaMallocAsync((void**)&cols, n * n_cols * 4, st), "vs_autotune_merkle alloc");
+  if (rc == VS_OK)
+    rc = check_cuda(cudaMallocAsync((void**)&scratch, merkle_scratch_words(n, MK_MAX_SPLIT) * 4, st), "vs_autotune_merkle alloc");
+  if (rc == VS_OK) rc = check_cuda(cudaMallocAsync((void**)&roots, 8 * (MK_MAX_SPLIT + 1) * 4, st), "vs_autotune_merkle alloc");
+  if (rc == VS_OK) rc = vs_fill_uniform_m31(cols, n * n_cols, 0x56530008ull, 0, stream);
+  if (rc == VS_OK) rc = check_cuda(cudaEventCreate(&e0), "vs_autotune_merkle event");
+  if (rc == VS_OK) rc = check_cuda(cudaEventCreate(&e1), "vs_autotune_merkle event");
+  uint32_t best_split = merkle_split();
+  float best_ms = 0.f;
+  for (uint32_t sp = 0; sp <= MK_MAX_SPLIT && rc == VS_OK; sp++) {
+    const LeafRowPacked leaf{cols, n, n_cols};
+    rc = merkle_root(leaf, n, roots + 8 * sp, st, scratch, sp);
+    if (rc == VS_OK) rc = check_cuda(cudaEventRecord(e0, st), "vs_autotune_merkle event");
+    for (uint32_t k = 0; k < reps && rc == VS_OK; k++) rc = merkle_root(leaf, n, roots + 8 * sp, st, scratch, sp);
+    if (rc == VS_OK) rc = check_cuda(cudaEventRecord(e1, st), "vs_autotune_merkle event");
+    if (rc == VS_OK) rc = check_cuda(cudaEventSynchronize(e1), "vs_autotune_merkle sync");
+    float ms = 0.f;
+    if (rc == VS_OK) rc = check_cuda(cudaEventElapsedTime(&ms, e0, e1), "vs_autotune_merkle time");
+    ms /= (float)reps;
+    if (ms_out && sp < cap) ms_out[sp] = ms;
+    if (rc == VS_OK && (sp == 0 || ms < best_ms)) {
+      best_ms = ms;
+      best_split = sp;
+    }
+  }
+  uint32_t h[8 * (MK_MAX_SPLIT + 1)];
+  if (rc == VS_OK) rc = check_cuda(cudaMemcpyAsync(h, roots, sizeof(h), cudaMemcpyDeviceToHost, st), "vs_autotune_merkle copy");
+  if (rc == VS_OK) rc = check_cuda(cudaStreamSynchronize(st), "vs_autotune_merkle sync");
+  for (uint32_t sp = 1; sp <= MK_MAX_SPLIT && rc == VS_OK; sp++)
+    if (memcmp(h, h + 8 * sp, 32) != 0) rc = set_error(VS_ERR_CUDA, "vs_autotune_merkle: split %u gave another root", sp);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (cols) cudaFreeAsync(cols, st);
+  if (scratch) cudaFreeAsync(scratch, st);
+  if (roots) cudaFreeAsync(roots, st);
+  if (rc != VS_OK) return rc;
+  g_merkle_split.store(best_split);
+  *best = best_split;
+  return check_cuda(cudaStreamSynchronize(st), "vs_autotune_merkle");
 }
 
 }  // extern "C"

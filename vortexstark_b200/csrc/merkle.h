@@ -12,39 +12,55 @@ namespace vs {
 // One level of parents: parents[i] = Blake2s(children[2i] || children[2i+1]).
 int launch_hash_nodes(const uint32_t* children, uint32_t* parents, uint64_t n_parents, cudaStream_t st);
 
+// stop_log (<= TL): 2^stop_log roots per tile instead of one (merkle_subtree_kernel).
 template <class Leaf>
-int merkle_tile_roots(const Leaf& leaf, uint64_t n_leaves, uint32_t TL, uint32_t* roots, cudaStream_t st) {
+int merkle_tile_roots(const Leaf& leaf, uint64_t n_leaves, uint32_t TL, uint32_t* roots, cudaStream_t st,
+                      uint32_t stop_log = 0) {
   const unsigned smem = merkle_smem_bytes(TL);  // at most 48 KiB (TL <= 10): no opt-in needed
   const uint64_t tiles = (n_leaves + (1ull << TL) - 1) >> TL;
-  merkle_subtree_kernel<Leaf><<<(unsigned)tiles, MK_THREADS, smem, st>>>(leaf, TL, n_leaves, roots);
+  if (stop_log > TL) stop_log = TL;
+  merkle_subtree_kernel<Leaf><<<(unsigned)tiles, MK_THREADS, smem, st>>>(leaf, TL, n_leaves, roots, stop_log);
   VS_LAUNCHED("merkle_subtree_kernel");
   return VS_OK;
 }
 
-// Words of scratch merkle_root needs for n_leaves leaves (0 when n_leaves <= 1024).
-inline uint64_t merkle_scratch_words(uint64_t n_leaves) {
-  uint64_t words = 0;
-  for (uint64_t cur = n_leaves >> MK_MAX_TL; n_leaves > (1ull << MK_MAX_TL) && cur > 1; cur >>= MK_MAX_TL) {
+// Largest split merkle_root accepts: the first level may stop at 2^8 roots per
+// 1024-leaf tile (the level where all 256 threads of a CTA still have a node).
+constexpr uint32_t MK_MAX_SPLIT = 8;
+// Process-wide split of the root-only trees (vs_merkle_split_set).
+uint32_t merkle_split();
+
+// Words of scratch merkle_root needs for n_leaves leaves with first-level split
+// `split` (0 when n_leaves <= 1024). Grows with split, so scratch sized for
+// MK_MAX_SPLIT serves every split.
+inline uint64_t merkle_scratch_words(uint64_t n_leaves, uint32_t split = 0) {
+  if (n_leaves <= (1ull << MK_MAX_TL)) return 0;
+  uint64_t cur = n_leaves >> (MK_MAX_TL - split);
+  uint64_t words = cur * 8;
+  while (cur > (1ull << MK_MAX_TL)) {
+    cur >>= MK_MAX_TL;
     words += cur * 8;
-    if (cur <= (1ull << MK_MAX_TL)) break;
   }
   return words;
 }
 
 // Root of a power-of-two tree whose leaves come from `leaf`. Intermediate tile
-// roots go to `scratch` (merkle_scratch_words(n_leaves) words; when null it is
-// allocated stream-ordered for the call). Each reduction level is written after
-// the previous one, never in place.
+// roots go to `scratch` (merkle_scratch_words(n_leaves, split) words; when null it
+// is allocated stream-ordered for the call). Each reduction level is written after
+// the previous one, never in place. The first level stops at 2^split roots per
+// 1024-leaf tile (split <= MK_MAX_SPLIT); the root is the same for every split.
 template <class Leaf>
-int merkle_root(const Leaf& leaf, uint64_t n_leaves, uint32_t* d_root, cudaStream_t st, uint32_t* scratch = nullptr) {
+int merkle_root(const Leaf& leaf, uint64_t n_leaves, uint32_t* d_root, cudaStream_t st, uint32_t* scratch = nullptr,
+                uint32_t split = 0) {
   if (!is_pow2(n_leaves)) return set_error(VS_ERR_INVALID, "merkle: leaf count %llu is not a power of two",
                                            (unsigned long long)n_leaves);
+  if (split > MK_MAX_SPLIT) return set_error(VS_ERR_INVALID, "merkle: split %u above %u", split, MK_MAX_SPLIT);
   const uint32_t L = ilog2(n_leaves);
   if (L <= MK_MAX_TL) return merkle_tile_roots(leaf, n_leaves, L, d_root, st);
   uint32_t* buf = scratch;
-  if (!buf) VS_CUDA(cudaMallocAsync((void**)&buf, merkle_scratch_words(n_leaves) * 4, st));
-  uint64_t cur = n_leaves >> MK_MAX_TL;
-  int rc = merkle_tile_roots(leaf, n_leaves, MK_MAX_TL, buf, st);
+  if (!buf) VS_CUDA(cudaMallocAsync((void**)&buf, merkle_scratch_words(n_leaves, split) * 4, st));
+  uint64_t cur = n_leaves >> (MK_MAX_TL - split);
+  int rc = merkle_tile_roots(leaf, n_leaves, MK_MAX_TL, buf, st, split);
   uint32_t* level = buf;
   while (rc == VS_OK) {
     const uint32_t Lc = ilog2(cur);

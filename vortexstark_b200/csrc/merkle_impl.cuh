@@ -25,9 +25,13 @@ constexpr int MK_MAX_TL = 10;
 // Shared memory: leaf layer (8 * 2^TL words) + next layer (8 * 2^(TL-1) words).
 inline unsigned merkle_smem_bytes(uint32_t TL) { return (8u << TL) * 4u + (TL ? (8u << (TL - 1)) * 4u : 0u); }
 
+// With stop_log > 0 the reduction stops at 2^stop_log subtree roots per tile
+// (written hash-major: hash j of tile b at roots[(b * 2^stop_log + j) * 8]), so a
+// CTA skips the narrow top levels of its tile, where most of its warps would wait
+// at barriers; the next reduction level takes them over.
 template <class Leaf>
 __global__ void __launch_bounds__(MK_THREADS) merkle_subtree_kernel(Leaf leaf, uint32_t TL, uint64_t n_leaves,
-                                                                   uint32_t* __restrict__ roots) {
+                                                                   uint32_t* __restrict__ roots, uint32_t stop_log) {
   extern __shared__ uint32_t mk_sm[];
   const uint32_t tile = 1u << TL;
   const uint64_t base = (uint64_t)blockIdx.x << TL;
@@ -47,7 +51,8 @@ __global__ void __launch_bounds__(MK_THREADS) merkle_subtree_kernel(Leaf leaf, u
   uint32_t* cur = bufA;
   uint32_t* nxt = bufB;
   uint32_t cur_n = tile;
-  while (cur_n > 1) {
+  const uint32_t n_out = 1u << stop_log;
+  while (cur_n > n_out) {
     const uint32_t half = cur_n >> 1;
     for (uint32_t i = threadIdx.x; i < half; i += MK_THREADS) {
       uint32_t m[16];
@@ -69,7 +74,8 @@ __global__ void __launch_bounds__(MK_THREADS) merkle_subtree_kernel(Leaf leaf, u
     nxt = t;
     cur_n = half;
   }
-  if (threadIdx.x < 8) roots[(uint64_t)blockIdx.x * 8 + threadIdx.x] = cur[threadIdx.x];
+  for (uint32_t i = threadIdx.x; i < 8 * n_out; i += MK_THREADS)
+    roots[((uint64_t)blockIdx.x * n_out + (i >> 3)) * 8 + (i & 7)] = cur[(i & 7) * n_out + (i >> 3)];
 }
 
 // ------------------------------------------------------------------ leaf functors
