@@ -463,6 +463,8 @@ def main():
     ap.add_argument("--slots", type=int, default=8, help="concurrent slots of the batched and served engines")
     ap.add_argument("--served-jobs", type=int, default=600)
     ap.add_argument("--no-autotune", action="store_true", help="keep the default NTT plans (no autotuning)")
+    ap.add_argument("--merkle-split", type=int, default=None,
+                    help="Merkle subtree split to use instead of tuning it (for profiler runs with --no-autotune)")
     ap.add_argument("--tune-sizes", type=int, nargs="*", default=list(range(16, 25)),
                     help="trace sizes (log) the NTT autotuner tunes before the timed runs")
     ap.add_argument("--prove-sizes", type=int, nargs="*", default=[20, 24, 28],
@@ -491,6 +493,8 @@ def main():
     # NTT launch shapes per size chosen by the autotuner before anything is timed
     # (34-column stwo LDEs); every later transform of a tuned size uses its plan.
     tuning = None
+    if args.merkle_split is not None:
+        api.set_merkle_split(args.merkle_split)
     if not args.no_autotune:
         tuning = {}
         for tl in sorted(set(args.tune_sizes) | {args.log_n}):
@@ -501,9 +505,10 @@ def main():
                                "default_plan": list(default), "default_ms": times.get(tuple(default)),
                                "candidates": len(times)}
         # Merkle subtree split of the root-only trees, tuned on the step's row-packed root
-        m = api.autotune_merkle(args.log_n + 2, n_cols=args.cols, reps=3)
-        tuning["merkle_split"] = {"split": m["best"], "ms_by_split": [round(x, 3) for x in m["ms"]],
-                                  "log_leaves": args.log_n + 2}
+        if args.merkle_split is None:
+            m = api.autotune_merkle(args.log_n + 2, n_cols=args.cols, reps=3)
+            tuning["merkle_split"] = {"split": m["best"], "ms_by_split": [round(x, 3) for x in m["ms"]],
+                                      "log_leaves": args.log_n + 2}
 
     n_cols, log_n, blow, fri_log, N, committed = workload(args)
     n = 1 << log_n
@@ -640,11 +645,12 @@ def main():
 
     # Roofline of the dominant kernel: merkle_subtree_kernel<LeafRowPacked> (the
     # largest single kernel of the step in the ncu launch list), timed by the events
-    # around the row-packed root (which also cover its 1024-to-1 upper reduction,
-    # under 0.3% of the phase). Algorithmic bytes: 4 * n_cols per leaf, each LDE
-    # word read once. Traffic: DRAM bytes per leaf from the ncu capture of the
-    # same kernel (34 columns, 2^22 leaves: 570.7 MB = 1.0004 x algorithmic),
-    # scaled to this launch's leaves. Per-phase HBM fractions are listed beside it;
+    # around the row-packed root (which also cover the upper reduction of its 2^split
+    # roots per tile, 3.6% of the phase at split 7). Algorithmic bytes: 4 * n_cols per
+    # leaf, each LDE word read once. Traffic: DRAM bytes per leaf from the ncu
+    # capture of the same kernel at split 7 (34 columns, 2^22 leaves: 570.5 MB read
+    # + 16.8 MB of subtree roots written = 1.0296 x algorithmic), scaled to this
+    # launch's leaves. Per-phase HBM fractions are listed beside it;
     # all phases are integer-ALU bound (Blake2s, M31 butterflies), not HBM bound.
     hbm = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0)) \
         if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
@@ -654,12 +660,13 @@ def main():
     ach = alg["merkle"] / (phase["merkle"] / 1e3) / 1e9
     roof = {"bound": "hbm", "kernel": "merkle_subtree_kernel<LeafRowPacked>", "achieved": ach, "peak": hbm,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)", "unit": "GB/s", "frac": ach / hbm,
-            "traffic": alg["merkle"] * 1.0004, "algorithmic_bytes": alg["merkle"],
-            # The binding resource is integer issue: instructions per launch (1286
-            # per Blake2s compression, the ncu count of this kernel; one
-            # compression per 64 B of leaf plus one per node) over 148 SMs x 4
-            # schedulers x 32 lanes x the sampled SM clock.
-            "int_issue_frac": (-(-n_cols * 4 // 64) + 1) * 1286 * N / (phase["merkle"] / 1e3)
+            "traffic": alg["merkle"] * 1.0296, "algorithmic_bytes": alg["merkle"],
+            # The binding resource is integer issue: instructions per launch (1248
+            # per Blake2s compression, the ncu count of this kernel: 633.8 M warp
+            # instructions for 2^22 leaves x 3.875 compressions; one compression per
+            # 64 B of leaf plus one per node) over 148 SMs x 4 schedulers x 32 lanes
+            # x the sampled SM clock.
+            "int_issue_frac": (-(-n_cols * 4 // 64) + 1) * 1248 * N / (phase["merkle"] / 1e3)
                               / (148 * 4 * 32 * clk_hz),
             "launch_ms": phase["merkle"], "phase_ms": phase,
             "phase_hbm_frac": {k: alg[k] / (phase[k] / 1e3) / 1e9 / hbm for k in phase}}
