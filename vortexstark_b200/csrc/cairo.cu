@@ -909,7 +909,7 @@ extern "C" int vs_cairo_oods_fri(void* channel, vs_cairo_oods_fri_io* io, vs_str
   // (prover.rs:2321-2381)
   uint32_t *fri = nullptr, *mscratch = nullptr;
   VS_TRY(s.alloc(&fri, 4 * N));
-  VS_TRY(s.alloc(&mscratch, merkle_scratch_words(N / 2, MK_MAX_SPLIT)));
+  VS_TRY(s.alloc(&mscratch, merkle_scratch_words_any(N / 2)));
   const uint32_t split = merkle_split();
   uint32_t* src[4] = {oq[0], oq[1], oq[2], oq[3]};
   uint32_t* dst[4];

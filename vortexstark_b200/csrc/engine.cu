@@ -49,7 +49,7 @@ struct CommitWs {
 
 uint64_t commit_bytes(uint32_t log_n, uint32_t n_cols) {
   const uint64_t n = 1ull << log_n, N = n << 2;
-  return (uint64_t)n_cols * (n + N) * 4 + merkle_scratch_words(N, MK_MAX_SPLIT) * 4 + 64;
+  return (uint64_t)n_cols * (n + N) * 4 + merkle_scratch_words_any(N) * 4 + 64;
 }
 
 // Jobs run at one of three stream priorities by working-set size (small jobs
@@ -123,7 +123,7 @@ struct Engine {
       VS_CUDA(cudaMalloc(&w->cols, (uint64_t)w->capacity * n * 4));
       VS_CUDA(cudaMalloc(&w->lde, (uint64_t)w->capacity * N * 4));
       VS_CUDA(cudaMalloc(&w->root, 32));
-      VS_CUDA(cudaMalloc(&w->scratch, std::max<uint64_t>(merkle_scratch_words(N, MK_MAX_SPLIT), 8) * 4));
+      VS_CUDA(cudaMalloc(&w->scratch, std::max<uint64_t>(merkle_scratch_words_any(N), 8) * 4));
       VS_CUDA(cudaMallocHost(&w->h_root, 32));
       w->bytes = commit_bytes(j.log_n, w->capacity);
       const TwiddleSet* t = nullptr;

@@ -80,7 +80,7 @@ int vs_fri_fold_commit(const uint32_t* d_src, uint32_t log_n, const uint32_t* h_
   if (log_n < 4 || log_n > 30) return set_error(VS_ERR_INVALID, "vs_fri_fold_commit: log_n %u out of range", log_n);
   const uint64_t N = 1ull << log_n;
   uint32_t* scratch = nullptr;
-  VS_CUDA(cudaMallocAsync((void**)&scratch, (merkle_scratch_words(N / 2, MK_MAX_SPLIT) + 8) * 4, st));
+  VS_CUDA(cudaMallocAsync((void**)&scratch, (merkle_scratch_words_any(N / 2) + 8) * 4, st));
   const uint32_t split = merkle_split();
   const uint32_t* src[4] = {d_src, d_src + N, d_src + 2 * N, d_src + 3 * N};
   uint32_t* bufs[2] = {d_work, d_work + 2 * N};  // each holds 4 planes of <= N/2 words

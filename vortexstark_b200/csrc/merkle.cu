@@ -186,7 +186,7 @@ int vs_autotune_merkle(uint32_t log_leaves, uint32_t n_cols, uint32_t reps, uint
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int rc = check_cuda(cudaMallocAsync((void**)&cols, n * n_cols * 4, st), "vs_autotune_merkle alloc");
   if (rc == VS_OK)
-    rc = check_cuda(cudaMallocAsync((void**)&scratch, merkle_scratch_words(n, MK_MAX_SPLIT) * 4, st), "vs_autotune_merkle alloc");
+    rc = check_cuda(cudaMallocAsync((void**)&scratch, merkle_scratch_words_any(n) * 4, st), "vs_autotune_merkle alloc");
   if (rc == VS_OK) rc = check_cuda(cudaMallocAsync((void**)&roots, 8 * (MK_MAX_SPLIT + 1) * 4, st), "vs_autotune_merkle alloc");
   if (rc == VS_OK) rc = vs_fill_uniform_m31(cols, n * n_cols, 0x56530008ull, 0, stream);
   if (rc == VS_OK) rc = check_cuda(cudaEventCreate(&e0), "vs_autotune_merkle event");

@@ -4,6 +4,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "merkle_impl.cuh"
 #include "vs_common.cuh"
 
@@ -30,18 +32,29 @@ constexpr uint32_t MK_MAX_SPLIT = 8;
 // Process-wide split of the root-only trees (vs_merkle_split_set).
 uint32_t merkle_split();
 
-// Words of scratch merkle_root needs for n_leaves leaves with first-level split
-// `split` (0 when n_leaves <= 1024). Grows with split, so scratch sized for
-// MK_MAX_SPLIT serves every split.
+// Split of a reduction level over `cur` hashes: the leaf level takes the split
+// as given; hash levels of at least 2^20 hashes (1024+ CTAs) take it too, smaller
+// ones reduce each tile to one root.
+inline uint32_t merkle_level_split(uint64_t cur, uint32_t split) { return cur >= (1ull << 20) ? split : 0u; }
+
+// Words of scratch merkle_root needs for n_leaves leaves with split `split` (0 when
+// n_leaves <= 1024): the sum of the hash levels it writes, in the order it writes
+// them (merkle_root follows the same sequence).
 inline uint64_t merkle_scratch_words(uint64_t n_leaves, uint32_t split = 0) {
   if (n_leaves <= (1ull << MK_MAX_TL)) return 0;
   uint64_t cur = n_leaves >> (MK_MAX_TL - split);
   uint64_t words = cur * 8;
   while (cur > (1ull << MK_MAX_TL)) {
-    cur >>= MK_MAX_TL;
+    cur >>= MK_MAX_TL - merkle_level_split(cur, split);
     words += cur * 8;
   }
   return words;
+}
+// Scratch that serves merkle_root at every split 0..MK_MAX_SPLIT.
+inline uint64_t merkle_scratch_words_any(uint64_t n_leaves) {
+  uint64_t w = 0;
+  for (uint32_t sp = 0; sp <= MK_MAX_SPLIT; sp++) w = std::max(w, merkle_scratch_words(n_leaves, sp));
+  return w;
 }
 
 // Root of a power-of-two tree whose leaves come from `leaf`. Intermediate tile
@@ -66,9 +79,10 @@ int merkle_root(const Leaf& leaf, uint64_t n_leaves, uint32_t* d_root, cudaStrea
     const uint32_t Lc = ilog2(cur);
     if (Lc <= MK_MAX_TL) { rc = merkle_tile_roots(LeafHashes{level}, cur, Lc, d_root, st); break; }
     uint32_t* next = level + cur * 8;
-    rc = merkle_tile_roots(LeafHashes{level}, cur, MK_MAX_TL, next, st);
+    const uint32_t sp = merkle_level_split(cur, split);
+    rc = merkle_tile_roots(LeafHashes{level}, cur, MK_MAX_TL, next, st, sp);
     level = next;
-    cur >>= MK_MAX_TL;
+    cur >>= MK_MAX_TL - sp;
   }
   if (!scratch) {
     cudaError_t e = cudaFreeAsync(buf, st);
