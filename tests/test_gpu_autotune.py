@@ -127,3 +127,23 @@ def test_autotune_merkle_keeps_a_split(L, default_split):
     res = api.autotune_merkle(16, n_cols=34, reps=2)
     assert 0 <= res["best"] <= 8 and api.merkle_split() == res["best"]
     assert all(t > 0 for t in res["ms"]) and res["ms"][res["best"]] == min(res["ms"])
+
+
+@pytest.mark.parametrize("split", [1, 5, 8])
+def test_prover_trees_with_split_match_oracle(L, default_split, split):
+    """Proof trees of 2^20 leaves (log_n 18) go through 2^min(split, 5) subtree
+    roots per tile in both provers; the bytes stay the oracle's."""
+    import ctypes as C
+    exp = O.prove(3, 77, 18)
+    api.set_merkle_split(split)
+    assert api.prove_fib(3, 77, 18) == exp
+    h = C.c_void_p()
+    V.check(L.vs_prover_create(18, C.byref(h)), "vs_prover_create")
+    try:
+        cap = 16 << 20
+        buf = (C.c_uint8 * cap)()
+        n = C.c_uint64()
+        V.check(L.vs_prover_prove(h, 3, 77, buf, cap, C.byref(n)), "vs_prover_prove")
+        assert bytes(buf[: n.value]) == exp
+    finally:
+        L.vs_prover_destroy(h)

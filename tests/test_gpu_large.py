@@ -32,3 +32,22 @@ def test_full_size_proof_matches_oracle_digest(key):
     assert len(plain) == c["len"]
     assert hashlib.sha256(plain).hexdigest() == c["sha256"]
     assert api.verify_fib(plain) == (True, "")
+
+
+@pytest.mark.parametrize("split", [3, 5])
+@pytest.mark.parametrize("key", sorted(CASES, key=lambda k: [int(x) for x in k.split(":")]))
+def test_full_size_proof_with_merkle_split(key, split):
+    """The prover's trees of 2^20+ leaves reach their tile roots through 2^split
+    subtree roots per tile; the proof bytes must not change."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    c = CASES[key]
+    api.set_merkle_split(split)
+    try:
+        plain = api.prove_fib(c["a"], c["b"], c["log_n"])
+        with api.Engine(1) as eng:
+            graph = eng.wait(eng.submit(api.fib_job(c["log_n"], c["a"], c["b"])))[0]
+    finally:
+        api.set_merkle_split(0)
+    assert graph == plain
+    assert hashlib.sha256(plain).hexdigest() == c["sha256"]

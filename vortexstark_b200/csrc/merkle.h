@@ -50,6 +50,22 @@ inline uint64_t merkle_scratch_words(uint64_t n_leaves, uint32_t split = 0) {
   }
   return words;
 }
+// Split used for trees that keep their 1024-leaf tile roots (prover trees of
+// 2^20+ leaves): tiles stop at 2^split subtree roots and `split` node launches
+// bring them up to the tile roots. Capped at 5, which bounds the extra scratch
+// at 2^5 + 2^4 hashes per tile (48 hashes per 1024 leaves).
+constexpr uint32_t MK_TILE_SPLIT_MAX = 5;
+inline uint32_t merkle_tile_split(uint64_t n_leaves) {
+  return n_leaves >= (1ull << 20) ? std::min<uint32_t>(merkle_split(), MK_TILE_SPLIT_MAX) : 0u;
+}
+// Tile roots of a 2^TL-leaf tiling through 2^sp subtree roots per tile: the
+// subtree kernel writes the subroots to sub_a, then sp node levels ping-pong
+// between sub_a (2^sp hashes per tile) and sub_b (2^(sp-1)) and end in `roots`.
+// Same tile roots as merkle_tile_roots(leaf, n, TL, roots).
+template <class Leaf>
+int merkle_tile_roots_split(const Leaf& leaf, uint64_t n_leaves, uint32_t TL, uint32_t sp, uint32_t* roots,
+                            uint32_t* sub_a, uint32_t* sub_b, cudaStream_t st);
+
 // Scratch that serves merkle_root at every split 0..MK_MAX_SPLIT.
 inline uint64_t merkle_scratch_words_any(uint64_t n_leaves) {
   uint64_t w = 0;
@@ -89,6 +105,23 @@ int merkle_root(const Leaf& leaf, uint64_t n_leaves, uint32_t* d_root, cudaStrea
     if (rc == VS_OK) rc = check_cuda(e, "merkle scratch free");
   }
   return rc;
+}
+
+template <class Leaf>
+int merkle_tile_roots_split(const Leaf& leaf, uint64_t n_leaves, uint32_t TL, uint32_t sp, uint32_t* roots,
+                            uint32_t* sub_a, uint32_t* sub_b, cudaStream_t st) {
+  if (!sp) return merkle_tile_roots(leaf, n_leaves, TL, roots, st);
+  const uint64_t tiles = n_leaves >> TL;
+  VS_TRY(merkle_tile_roots(leaf, n_leaves, TL, sub_a, st, sp));
+  uint32_t* src = sub_a;
+  uint64_t c = tiles << sp;
+  for (uint32_t k = sp; k > 1; k--) {
+    uint32_t* dst = src == sub_a ? sub_b : sub_a;
+    VS_TRY(launch_hash_nodes(src, dst, c / 2, st));
+    src = dst;
+    c /= 2;
+  }
+  return launch_hash_nodes(src, roots, tiles, st);
 }
 
 }  // namespace vs

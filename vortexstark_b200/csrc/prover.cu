@@ -193,7 +193,13 @@ static int commit_tree(const Leaf& leaf, uint64_t n, DevTree& t, DevMem& mem, cu
   uint64_t cnt = n >> t.TL;
   uint32_t* l0 = nullptr;
   VS_TRY(mem.alloc(&l0, cnt * 8));
-  VS_TRY(merkle_tile_roots(leaf, n, t.TL, l0, st));
+  const uint32_t sp = t.TL == MK_MAX_TL ? merkle_tile_split(n) : 0u;
+  uint32_t *sub_a = nullptr, *sub_b = nullptr;
+  if (sp) {
+    VS_TRY(mem.alloc(&sub_a, (cnt << sp) * 8));
+    VS_TRY(mem.alloc(&sub_b, (cnt << (sp - 1)) * 8));
+  }
+  VS_TRY(merkle_tile_roots_split(leaf, n, t.TL, sp, l0, sub_a, sub_b, st));
   t.layers.push_back(l0);
   while (cnt > 1) {
     uint32_t* par = nullptr;

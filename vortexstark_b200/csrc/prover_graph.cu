@@ -247,6 +247,8 @@ struct GraphProver::Impl {
   std::vector<std::array<uint32_t*, 4>> fri_vals;
   TreeBufs trace_t, quot_t;
   std::vector<TreeBufs> fri_t;
+  // subroot scratch shared by the trees (committed one after another in the graph)
+  uint32_t split = 0, *sub_a = nullptr, *sub_b = nullptr;
   // arena layout (words)
   size_t a_roots = 0, a_last = 0, a_q = 0, a_tv = 0, a_qv = 0, a_fv = 0, a_paths = 0, words = 0;
   std::vector<size_t> a_tree;  // path region per tree: trace, quot, fri...
@@ -288,7 +290,8 @@ struct GraphProver::Impl {
   }
   template <class Leaf>
   int commit(const Leaf& leaf, TreeBufs& t) {
-    VS_TRY(merkle_tile_roots(leaf, t.n, t.TL, t.layers[0], st));
+    const uint32_t sp = (t.TL == MK_MAX_TL && t.n >= (1ull << 20)) ? split : 0u;
+    VS_TRY(merkle_tile_roots_split(leaf, t.n, t.TL, sp, t.layers[0], sub_a, sub_b, st));
     for (size_t k = 1; k < t.layers.size(); k++)
       VS_TRY(launch_hash_nodes(t.layers[k - 1], t.layers[k], t.n >> (t.TL + k), st));
     return VS_OK;
@@ -325,6 +328,11 @@ struct GraphProver::Impl {
     VS_TRY(alloc(&d_ch, 1));
     VS_TRY(tree_bufs(trace_t, N));
     VS_TRY(tree_bufs(quot_t, N));
+    split = merkle_tile_split(N);  // fixed for the prover's lifetime (its graph is captured once)
+    if (split) {
+      VS_TRY(alloc(&sub_a, ((N >> MK_MAX_TL) << split) * 8));
+      VS_TRY(alloc(&sub_b, ((N >> MK_MAX_TL) << (split - 1)) * 8));
+    }
     fri_t.resize(nf);
     for (uint32_t l = 0; l < nf; l++) {
       const uint64_t half = N >> (l + 1);
