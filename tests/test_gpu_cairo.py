@@ -314,3 +314,20 @@ def test_tile_tree_paths_rejects_bad_arguments(L):
     assert L.vs_tile_tree_paths(1, hc, 3, 6, ptr(t), ix, 1, out, out, None) != 0   # SoA4 needs 4 columns
     assert L.vs_tile_tree_paths(0, hc, 4, 6, ptr(t), ix, 1, out, out, None) != 0   # index out of range
     assert L.vs_tile_tree_paths(7, hc, 4, 6, ptr(t), ix, 0, out, out, None) != 0   # unknown leaf
+
+
+@pytest.mark.parametrize("split", [0, 5])
+def test_group_commit_tile_roots_with_split(L, split):
+    """2^20 evaluation rows: the tile roots go through 2^split subtree roots per tile
+    when a split is set; roots and tile roots stay the oracle's."""
+    from vortexstark_b200 import api
+    log_n, nc = 18, 2
+    n = 1 << log_n
+    cols = np.stack([O.seeded_m31(0x7300 + c, n) for c in range(nc)])
+    blind = [12345, 0]
+    api.set_merkle_split(split)
+    try:
+        got = run_group(L, cols, log_n, blind)
+    finally:
+        api.set_merkle_split(0)
+    check(got, O.commit_group_cairo(cols, log_n, blind))

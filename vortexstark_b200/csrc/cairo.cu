@@ -566,6 +566,22 @@ int eval_at_points(const uint32_t* const* h_cols, uint32_t n_cols, uint32_t L, c
   return VS_OK;
 }
 
+// 1024-leaf tile roots of a commitment, through 2^split subtree roots per tile
+// (merkle_tile_split) for trees of 2^20+ leaves; stream-ordered subroot scratch.
+template <class Leaf>
+int tile_roots_split(const Leaf& leaf, uint64_t N, uint32_t* tiles, cudaStream_t st) {
+  const uint32_t sp = merkle_tile_split(N);
+  if (!sp) return merkle_tile_roots(leaf, N, MK_MAX_TL, tiles, st);
+  const uint64_t t = N >> MK_MAX_TL;
+  uint32_t *a = nullptr, *b = nullptr;
+  VS_CUDA(cudaMallocAsync((void**)&a, (t << sp) * 32, st));
+  int rc = check_cuda(cudaMallocAsync((void**)&b, (t << (sp - 1)) * 32, st), "subroot scratch");
+  if (rc == VS_OK) rc = merkle_tile_roots_split(leaf, N, MK_MAX_TL, sp, tiles, a, b, st);
+  cudaFreeAsync(a, st);
+  if (b) cudaFreeAsync(b, st);
+  return rc;
+}
+
 }  // namespace vs
 
 using namespace vs;
@@ -626,7 +642,7 @@ extern "C" int vs_commit_group_cairo(const uint32_t* d_cols_hc, uint64_t col_str
     } else {
       uint32_t* tiles = d_tile_roots;
       if (!tiles) rc = check_cuda(cudaMallocAsync((void**)&tiles, (N / 1024) * 32, st), "tile roots");
-      if (rc == VS_OK) rc = merkle_tile_roots(leaf, N, 10, tiles, st);
+      if (rc == VS_OK) rc = tile_roots_split(leaf, N, tiles, st);
       if (rc == VS_OK) rc = merkle_root(LeafHashes{tiles}, N / 1024, d_root, st);
       if (!d_tile_roots && tiles) cudaFreeAsync(tiles, st);
     }
@@ -666,7 +682,7 @@ int commit_soa4_tiles(uint32_t* const c[4], uint64_t N, uint32_t* d_root, uint32
     VS_CUDA(cudaMemcpyAsync(tiles, d_root, 32, cudaMemcpyDeviceToDevice, st));
     return VS_OK;
   }
-  VS_TRY(merkle_tile_roots(leaf, N, 10, tiles, st));
+  VS_TRY(tile_roots_split(leaf, N, tiles, st));
   return merkle_root(LeafHashes{tiles}, N / 1024, d_root, st);
 }
 int read_hash(const uint32_t* d, h::Hash& out, cudaStream_t st) {
