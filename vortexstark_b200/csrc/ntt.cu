@@ -463,23 +463,26 @@ __device__ __forceinline__ void bfly4(uint4& a, uint4& b, uint32_t tt) {
   bfly<FWD>(a.w, b.w, tt);
 }
 
-// Butterflies of chunk round r; layer q of the round (tile bit p = P0 + q) is
-// global layer a + p - C with group index h = hi * 2^(T-1-p) + (address >> (p+1)).
-// Twiddle tables are 16-byte aligned up to their size (host-checked), as for rbfly.
-template <bool FWD, int M, int C, int r, int S0 = C>
-__device__ __forceinline__ void rbfly4(uint4 (&v)[8], const TileGeo& g, const NttTw& tw) {
+
+// Twiddles of chunk round r for every subgroup of the thread, doubled (for
+// mul_tt): layer q of subgroup s at t[s * (K - 1) + K - (K >> q) + gg]. Split from
+// the butterflies so a round's twiddles can be fetched one round ahead. A
+// thread's twiddles of one layer are consecutive and start at a multiple of their
+// count; tables are 16-byte aligned up to their size (host-checked), so they load
+// as one 128-, 64- or 32-bit access per layer.
+template <int M, int C, int r, int S0 = C>
+__device__ __forceinline__ void tw4_fetch(uint32_t (&t)[8], const TileGeo& g, const NttTw& tw) {
   using S = Tile4<M, C, S0>;
   constexpr int P0 = S::P0(r), R = S::R(r), K = 1 << R, SUB = 1 << (3 - R), T = S::T;
 #pragma unroll
   for (int s = 0; s < SUB; s++) {
     const uint32_t base = ins4<P0, R>(threadIdx.x + s * S::NT, 0);
-    uint32_t t[K];  // layer q's twiddles at t[K - (K >> q) + gg]
 #pragma unroll
     for (int q = 0; q < R; q++) {
       const int p = P0 + q;
       const uint32_t hb = (g.hi << (T - 1 - p)) | (base >> (p + 1));
       const uint32_t* tp = tw.layer[g.a + p - C] + hb;
-      const int cnt = K >> (q + 1), o = K - (K >> q);
+      const int cnt = K >> (q + 1), o = s * (K - 1) + K - (K >> q);
       if (cnt == 4) {
         const uint4 w = __ldg(reinterpret_cast<const uint4*>(tp));
         t[o] = w.x << 1;
@@ -494,12 +497,20 @@ __device__ __forceinline__ void rbfly4(uint4 (&v)[8], const TileGeo& g, const Nt
         t[o] = __ldg(tp) << 1;
       }
     }
+  }
+}
+template <bool FWD, int M, int C, int r, int S0 = C>
+__device__ __forceinline__ void rbfly4_t(uint4 (&v)[8], const uint32_t (&t)[8]) {
+  using S = Tile4<M, C, S0>;
+  constexpr int R = S::R(r), K = 1 << R, SUB = 1 << (3 - R);
+#pragma unroll
+  for (int s = 0; s < SUB; s++)
 #pragma unroll
     for (int qq = 0; qq < R; qq++) {
       const int q = FWD ? R - 1 - qq : qq;
 #pragma unroll
       for (int gg = 0; gg < (K >> (q + 1)); gg++) {
-        const uint32_t tv = t[K - (K >> q) + gg];
+        const uint32_t tv = t[s * (K - 1) + K - (K >> q) + gg];
 #pragma unroll
         for (int l = 0; l < (1 << q); l++) {
           const int k0 = (gg << (q + 1)) | l;
@@ -507,14 +518,110 @@ __device__ __forceinline__ void rbfly4(uint4 (&v)[8], const TileGeo& g, const Nt
         }
       }
     }
+}
+
+// Inverse chunk rounds r..TOP with round r's twiddles in t; each round fetches
+// the next round's twiddles before its own shared-memory loads. The last round
+// applies `scale` (if nonzero) and stores to cf (the coefficient tile of the LDE
+// top pass; the working tile itself in a pass kernel).
+template <int M, int C, int r, int S0 = C>
+__device__ __forceinline__ void inv_rounds4(uint32_t* sm, uint32_t* cf, const TileGeo& g, const NttTw& tw,
+                                            uint32_t scale, uint32_t (&t)[8]) {
+  constexpr int TOP = Tile4<M, C, S0>::NR - 1;
+  uint32_t tn[8];
+  if constexpr (r < TOP) tw4_fetch<M, C, r + 1, S0>(tn, g, tw);
+  uint4 v[8];
+  rload4<M, C, r, S0>(v, sm);
+  rbfly4_t<false, M, C, r, S0>(v, t);
+  if constexpr (r == TOP) {
+    if (scale) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        v[k].x = mul(v[k].x, scale);
+        v[k].y = mul(v[k].y, scale);
+        v[k].z = mul(v[k].z, scale);
+        v[k].w = mul(v[k].w, scale);
+      }
+    }
+    rstore4<M, C, r, S0>(v, cf);
+  } else {
+    rstore4<M, C, r, S0>(v, sm);
+  }
+  __syncthreads();
+  if constexpr (r < TOP) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) t[k] = tn[k];
+    inv_rounds4<M, C, r + 1, S0>(sm, cf, g, tw, scale, t);
+  }
+}
+// Forward chunk rounds r..0 (round TOP reads from cf: the parked coefficients of
+// the LDE top pass, the working tile in a pass kernel), twiddles fetched one round
+// ahead as above.
+template <int M, int C, int r, int S0 = C>
+__device__ __forceinline__ void fwd_rounds4(uint32_t* sm, const uint32_t* cf, const TileGeo& g, const NttTw& tw,
+                                            uint32_t (&t)[8]) {
+  constexpr int TOP = Tile4<M, C, S0>::NR - 1;
+  uint32_t tn[8];
+  if constexpr (r > 0) tw4_fetch<M, C, (r > 0 ? r - 1 : 0), S0>(tn, g, tw);
+  uint4 v[8];
+  rload4<M, C, r, S0>(v, r == TOP ? cf : sm);
+  rbfly4_t<true, M, C, r, S0>(v, t);
+  rstore4<M, C, r, S0>(v, sm);  // the previous block's tile_store finished before the block-end barrier
+  __syncthreads();
+  if constexpr (r > 0) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) t[k] = tn[k];
+    fwd_rounds4<M, C, (r > 0 ? r - 1 : 0), S0>(sm, cf, g, tw, t);
   }
 }
 
-template <bool FWD, int M, int C, int r, int S0 = C>
-__device__ __forceinline__ void round4(uint32_t* sm, const TileGeo& g, const NttTw& tw, uint32_t scale = 0) {
+// Same dataflow as ntt_lde_top_kernel: inverse rounds with the 1/n scale folded
+// into the last one, which parks the coefficients in the second tile; then for
+// each blowup block q the forward rounds from the parked tile, stored to block q.
+// Each round's twiddles are loaded during the round before it (the first inverse
+// round's during the tile load, a block's first forward round's during the
+// previous block's tile store), so their L2 latency is off the round's critical path.
+template <int M, int C>
+__global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPass inv, NttPass fwd, uint32_t B) {
+  using S = Tile4<M, C>;
+  static_assert(S::NR <= 4, "at most four chunk rounds");
+  constexpr int TOP = S::NR - 1;
+  extern __shared__ __align__(16) uint32_t lde4_sm[];
+  uint32_t* sm = lde4_sm;            // working tile
+  uint32_t* cf = lde4_sm + S::SIZE;  // coefficients
+  const TileGeo gi = tile_geo<M, C>(inv.a, blockIdx.x);
+  uint32_t t[8];
+  tw4_fetch<M, C, 0>(t, gi, inv.tw);
+  tile_load4<M, C>(sm, col_src(inv, blockIdx.y), gi, inv.src_mask);
+  __syncthreads();
+  inv_rounds4<M, C, 0>(sm, cf, gi, inv.tw, inv.scale, t);
+  uint32_t* dst = col_dst(fwd, blockIdx.y);
+  TileGeo gf = gi;
+  gf.hi = 0;
+  gf.gbase = gi.gbase;
+  tw4_fetch<M, C, TOP>(t, gf, fwd.tw);
+  for (uint32_t q = 0; q < (1u << B); q++) {
+    fwd_rounds4<M, C, TOP>(sm, cf, gf, fwd.tw, t);
+    const TileGeo gq = gf;
+    if (q + 1 < (1u << B)) {
+      gf.hi = q + 1;
+      gf.gbase = ((q + 1) << (gi.a + M)) | gi.gbase;
+      tw4_fetch<M, C, TOP>(t, gf, fwd.tw);
+    }
+    tile_store4<M, C>(sm, dst, gq);
+    __syncthreads();
+  }
+}
+
+// One chunk round of a pass: shared-memory loads, then the round's twiddles, then
+// the butterflies (and the inverse scale on the last round).
+template <bool FWD, int M, int C, int r, int S0>
+__device__ __forceinline__ void round4(uint32_t* sm, const TileGeo& g, const NttTw& tw, uint32_t scale) {
   uint4 v[8];
+  uint32_t t[8];
   rload4<M, C, r, S0>(v, sm);
-  rbfly4<FWD, M, C, r, S0>(v, g, tw);
+  tw4_fetch<M, C, r, S0>(t, g, tw);
+  rbfly4_t<FWD, M, C, r, S0>(v, t);
   if (scale) {
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -526,66 +633,14 @@ __device__ __forceinline__ void round4(uint32_t* sm, const TileGeo& g, const Ntt
   }
   rstore4<M, C, r, S0>(v, sm);
 }
-// Rounds [lo, hi] in transform order (forward: hi down to lo), barrier after each.
-template <bool FWD, int M, int C>
-__device__ __forceinline__ void rounds4(uint32_t* sm, const TileGeo& g, const NttTw& tw, int lo, int hi) {
-  using S = Tile4<M, C>;
-#pragma unroll
-  for (int i = 0; i < S::NR; i++) {
-    const int r = FWD ? S::NR - 1 - i : i;
-    if (r < lo || r > hi) continue;
-    switch (r) {
-      case 0: round4<FWD, M, C, 0>(sm, g, tw); break;
-      case 1: round4<FWD, M, C, (S::NR > 1 ? 1 : 0)>(sm, g, tw); break;
-      case 2: round4<FWD, M, C, (S::NR > 2 ? 2 : 0)>(sm, g, tw); break;
-      default: round4<FWD, M, C, (S::NR > 3 ? 3 : 0)>(sm, g, tw); break;
-    }
-    __syncthreads();
-  }
-}
-
-// Same dataflow as ntt_lde_top_kernel: inverse rounds with the 1/n scale folded
-// into the last one, which parks the coefficients in the second tile; then for
-// each blowup block q the forward rounds from the parked tile, stored to block q.
-template <int M, int C>
-__global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPass inv, NttPass fwd, uint32_t B) {
-  using S = Tile4<M, C>;
-  static_assert(S::NR <= 4, "at most four chunk rounds");
-  constexpr int TOP = S::NR - 1;
-  extern __shared__ __align__(16) uint32_t lde4_sm[];
-  uint32_t* sm = lde4_sm;            // working tile
-  uint32_t* cf = lde4_sm + S::SIZE;  // coefficients
-  const TileGeo gi = tile_geo<M, C>(inv.a, blockIdx.x);
-  tile_load4<M, C>(sm, col_src(inv, blockIdx.y), gi, inv.src_mask);
-  __syncthreads();
-  rounds4<false, M, C>(sm, gi, inv.tw, 0, TOP - 1);
-  {
-    uint4 v[8];
-    rload4<M, C, TOP>(v, sm);
-    rbfly4<false, M, C, TOP>(v, gi, inv.tw);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      v[k].x = mul(v[k].x, inv.scale);
-      v[k].y = mul(v[k].y, inv.scale);
-      v[k].z = mul(v[k].z, inv.scale);
-      v[k].w = mul(v[k].w, inv.scale);
-    }
-    rstore4<M, C, TOP>(v, cf);
-  }
-  __syncthreads();
-  uint32_t* dst = col_dst(fwd, blockIdx.y);
-  for (uint32_t q = 0; q < (1u << B); q++) {
-    TileGeo gf = gi;
-    gf.hi = q;
-    gf.gbase = (q << (gi.a + M)) | gi.gbase;
-    uint4 v[8];
-    rload4<M, C, TOP>(v, cf);
-    rbfly4<true, M, C, TOP>(v, gf, fwd.tw);
-    rstore4<M, C, TOP>(v, sm);  // the previous block's tile_store finished before the loop-end barrier
-    __syncthreads();
-    rounds4<true, M, C>(sm, gf, fwd.tw, 0, TOP - 1);
-    tile_store4<M, C>(sm, dst, gf);
-    __syncthreads();
+template <bool FWD, int M, int C, int S0>
+__device__ __forceinline__ void chunk_round(int r, uint32_t* sm, const TileGeo& g, const NttTw& tw, uint32_t scale) {
+  using S4 = Tile4<M, C, S0>;
+  switch (r) {
+    case 0: round4<FWD, M, C, 0, S0>(sm, g, tw, scale); break;
+    case 1: round4<FWD, M, C, (S4::NR > 1 ? 1 : 0), S0>(sm, g, tw, scale); break;
+    case 2: round4<FWD, M, C, (S4::NR > 2 ? 2 : 0), S0>(sm, g, tw, scale); break;
+    default: round4<FWD, M, C, (S4::NR > 3 ? 3 : 0), S0>(sm, g, tw, scale); break;
   }
 }
 
@@ -602,16 +657,6 @@ __device__ __forceinline__ void tile_load_async4(uint32_t* sm, const uint32_t* _
   for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
     const uint32_t e = 4 * (threadIdx.x + i * S::NT);
     cp_async16(base + 4 * swz<0>(e), src + (gidx<M, C>(g, e) & mask));
-  }
-}
-template <bool FWD, int M, int C, int S0>
-__device__ __forceinline__ void chunk_round(int r, uint32_t* sm, const TileGeo& g, const NttTw& tw, uint32_t scale) {
-  using S4 = Tile4<M, C, S0>;
-  switch (r) {
-    case 0: round4<FWD, M, C, 0, S0>(sm, g, tw, scale); break;
-    case 1: round4<FWD, M, C, (S4::NR > 1 ? 1 : 0), S0>(sm, g, tw, scale); break;
-    case 2: round4<FWD, M, C, (S4::NR > 2 ? 2 : 0), S0>(sm, g, tw, scale); break;
-    default: round4<FWD, M, C, (S4::NR > 3 ? 3 : 0), S0>(sm, g, tw, scale); break;
   }
 }
 template <bool FWD, int M, int C>
@@ -636,6 +681,8 @@ __global__ void __launch_bounds__(1 << (M + C - 5), (M + C == 13) ? 3 : 2) ntt_p
     cp_async_wait1();
     __syncthreads();
     const TileGeo g = tile_geo<M, C>(p.a, w / n_cols);
+    // (fetching a round's twiddles one round ahead, as the LDE top pass does,
+    // measured slower here: the double-buffered tiles already hide the latency)
     if (!FWD) {
       if (C == 0) {
         round_sm<false, M, C, 0>(sm, g, p.tw, 0);
