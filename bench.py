@@ -370,6 +370,15 @@ def proof_workloads(args):
         for j in W.shapes(jobs):
             eng.prepare(api.commit_job(j.log_n, 34, 0) if j.kind == api.COMMIT else j)
 
+    # Start from an empty stream-ordered pool: the step, e2e and Cairo runs above
+    # leave GBs of differently sized blocks cached in it (release threshold = all),
+    # which slowed the plain path's per-call allocations twofold. A threshold of 0
+    # releases them at the next synchronisation; then the pool keeps everything again.
+    import torch
+    api.init_memory_pool(0)
+    torch.cuda.synchronize()
+    api.init_memory_pool((1 << 64) - 1)
+
     out = {}
     plain = W.plain_jobs(64, 16)
     W.run_plain(plain[:4])
