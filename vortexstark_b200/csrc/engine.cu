@@ -139,7 +139,8 @@ struct Engine {
   uint64_t job_bytes(const vs_job& j) {
     if (j.kind == VS_JOB_COMMIT) return commit_bytes(j.log_n, j.n_cols);
     const uint64_t N = 1ull << (j.log_n + 2);
-    return (1ull << j.log_n) * 4 + N * 4 * 3 + N * 16 + (16u << 20);
+    return (1ull << j.log_n) * 4 + N * 4 * 3 + N * 16 + (16u << 20) +
+           merkle_tile_scratch_bytes(N, N >= (1ull << 20) ? MK_TILE_SPLIT_MAX : 0u);
   }
 
   int run_job(Slot& s, const vs_job& j, std::vector<uint8_t>& out) {

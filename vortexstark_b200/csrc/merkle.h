@@ -58,6 +58,10 @@ constexpr uint32_t MK_TILE_SPLIT_MAX = 5;
 inline uint32_t merkle_tile_split(uint64_t n_leaves) {
   return n_leaves >= (1ull << 20) ? std::min<uint32_t>(merkle_split(), MK_TILE_SPLIT_MAX) : 0u;
 }
+// Subroot scratch of a tile-root tree of n_leaves leaves at split sp (0: none).
+inline uint64_t merkle_tile_scratch_bytes(uint64_t n_leaves, uint32_t sp) {
+  return sp ? ((n_leaves >> MK_MAX_TL) << sp) * 32 + ((n_leaves >> MK_MAX_TL) << (sp - 1)) * 32 : 0;
+}
 // Tile roots of a 2^TL-leaf tiling through 2^sp subtree roots per tile: the
 // subtree kernel writes the subroots to sub_a, then sp node levels ping-pong
 // between sub_a (2^sp hashes per tile) and sub_b (2^(sp-1)) and end in `roots`.

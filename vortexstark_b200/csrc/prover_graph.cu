@@ -483,6 +483,7 @@ uint64_t GraphProver::device_bytes() const {
   uint64_t b = 0;
   b += impl->n * 4 + impl->N * 4 * 3 + impl->words * 4;  // trace, eval, tile levels (<N/2 words each), arena
   for (uint32_t l = 0; l < impl->nf; l++) b += (impl->N >> (l + 1)) * 16;
+  b += merkle_tile_scratch_bytes(impl->N, impl->split);
   return b;
 }
 int GraphProver::launch(uint32_t a, uint32_t b, cudaStream_t on) {
