@@ -655,11 +655,11 @@ def main():
     # Roofline of the dominant kernel: merkle_subtree_kernel<LeafRowPacked> (the
     # largest single kernel of the step in the ncu launch list), timed by the events
     # around the row-packed root (which also cover the upper reduction of its 2^split
-    # roots per tile, 3.6% of the phase at split 7). Algorithmic bytes: 4 * n_cols per
-    # leaf, each LDE word read once. Traffic: DRAM bytes per leaf from the ncu
-    # capture of the same kernel at split 7 (34 columns, 2^22 leaves: 570.5 MB read
-    # + 16.8 MB of subtree roots written = 1.0296 x algorithmic), scaled to this
-    # launch's leaves. Per-phase HBM fractions are listed beside it;
+    # roots per tile). Algorithmic bytes: 4 * n_cols per leaf, each LDE word read
+    # once. Traffic: the ncu capture of the same kernel (34 columns, 2^22 leaves,
+    # split 7) read 570.5 MB = 1.0002 x algorithmic and wrote exactly its subtree
+    # roots (2^split hashes of 32 B per 1024-leaf tile, 16.8 MB); the same per-leaf
+    # read ratio plus the roots at this run's split. Per-phase HBM fractions are listed beside it;
     # all phases are integer-ALU bound (Blake2s, M31 butterflies), not HBM bound.
     hbm = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0)) \
         if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
@@ -669,7 +669,8 @@ def main():
     ach = alg["merkle"] / (phase["merkle"] / 1e3) / 1e9
     roof = {"bound": "hbm", "kernel": "merkle_subtree_kernel<LeafRowPacked>", "achieved": ach, "peak": hbm,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)", "unit": "GB/s", "frac": ach / hbm,
-            "traffic": alg["merkle"] * 1.0296, "algorithmic_bytes": alg["merkle"],
+            "traffic": alg["merkle"] * 1.0002 + (N >> 10 << api.merkle_split()) * 32,
+            "algorithmic_bytes": alg["merkle"],
             # The binding resource is integer issue: instructions per launch (1248
             # per Blake2s compression, the ncu count of this kernel: 633.8 M warp
             # instructions for 2^22 leaves x 3.875 compressions; one compression per
