@@ -27,7 +27,26 @@ __device__ __forceinline__ uint32_t pow(uint32_t a, uint32_t e) {
   while (e) { if (e & 1) r = mul(r, a); a = mul(a, a); e >>= 1; }
   return r;
 }
-__device__ __forceinline__ uint32_t inv(uint32_t a) { return pow(a, VS_P - 2); }  // 0 -> 0
+// a^(p-2) = a^(2^31 - 3) (Fermat; 0 -> 0) by a fixed addition chain: 30 squarings
+// and 8 multiplications instead of square-and-multiply's 31 + 30.
+//   e_k = a^(2^k - 1):  e2 = e1^2 e1, e4 = e2^(2^2) e2, e8 = e4^(2^4) e4,
+//   e16 = e8^(2^8) e8, e24 = e16^(2^8) e8, e28 = e24^(2^4) e4, e29 = e28^2 a,
+//   a^(p-2) = e29^(2^2) a   since (2^29 - 1) * 4 + 1 = 2^31 - 3.
+__device__ __forceinline__ uint32_t sqn(uint32_t x, int n) {
+#pragma unroll
+  for (int i = 0; i < n; i++) x = mul(x, x);
+  return x;
+}
+__device__ __forceinline__ uint32_t inv(uint32_t a) {
+  const uint32_t e2 = mul(sqn(a, 1), a);
+  const uint32_t e4 = mul(sqn(e2, 2), e2);
+  const uint32_t e8 = mul(sqn(e4, 4), e4);
+  const uint32_t e16 = mul(sqn(e8, 8), e8);
+  const uint32_t e24 = mul(sqn(e16, 8), e8);
+  const uint32_t e28 = mul(sqn(e24, 4), e4);
+  const uint32_t e29 = mul(sqn(e28, 1), a);
+  return mul(sqn(e29, 2), a);
+}
 
 struct cm31 { uint32_t a, b; };
 __device__ __forceinline__ cm31 cadd(cm31 x, cm31 y) { return {add(x.a, y.a), add(x.b, y.b)}; }
