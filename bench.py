@@ -657,8 +657,8 @@ def main():
     # around the row-packed root (which also cover the upper reduction of its 2^split
     # roots per tile). Algorithmic bytes: 4 * n_cols per leaf, each LDE word read
     # once. Traffic: the ncu capture of the same kernel (34 columns, 2^22 leaves,
-    # split 7) read 570.5 MB = 1.0002 x algorithmic and wrote exactly its subtree
-    # roots (2^split hashes of 32 B per 1024-leaf tile, 16.8 MB); the same per-leaf
+    # split 8) read 570.6 MB = 1.0004 x algorithmic and wrote its subtree roots
+    # (2^split hashes of 32 B per 1024-leaf tile, 33.6 MB); the same per-leaf
     # read ratio plus the roots at this run's split. Per-phase HBM fractions are listed beside it;
     # all phases are integer-ALU bound (Blake2s, M31 butterflies), not HBM bound.
     hbm = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0)) \
@@ -669,14 +669,14 @@ def main():
     ach = alg["merkle"] / (phase["merkle"] / 1e3) / 1e9
     roof = {"bound": "hbm", "kernel": "merkle_subtree_kernel<LeafRowPacked>", "achieved": ach, "peak": hbm,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)", "unit": "GB/s", "frac": ach / hbm,
-            "traffic": alg["merkle"] * 1.0002 + (N >> 10 << api.merkle_split()) * 32,
+            "traffic": alg["merkle"] * 1.0004 + (N >> 10 << api.merkle_split()) * 32,
             "algorithmic_bytes": alg["merkle"],
-            # The binding resource is integer issue: instructions per launch (1248
-            # per Blake2s compression, the ncu count of this kernel: 633.8 M warp
-            # instructions for 2^22 leaves x 3.875 compressions; one compression per
-            # 64 B of leaf plus one per node) over 148 SMs x 4 schedulers x 32 lanes
-            # x the sampled SM clock.
-            "int_issue_frac": (-(-n_cols * 4 // 64) + 1) * 1248 * N / (phase["merkle"] / 1e3)
+            # The binding resource is integer issue: instructions per launch (1179
+            # per Blake2s compression on average, the ncu count of this kernel at
+            # split 8: 579.4 M warp instructions for 2^22 leaves x 3.75 compressions;
+            # one compression per 64 B of leaf plus one per node) over 148 SMs x 4
+            # schedulers x 32 lanes x the sampled SM clock.
+            "int_issue_frac": (-(-n_cols * 4 // 64) + 1) * 1179 * N / (phase["merkle"] / 1e3)
                               / (148 * 4 * 32 * clk_hz),
             "launch_ms": phase["merkle"], "phase_ms": phase,
             "phase_hbm_frac": {k: alg[k] / (phase[k] / 1e3) / 1e9 / hbm for k in phase}}
