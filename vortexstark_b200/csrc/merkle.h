@@ -33,9 +33,12 @@ constexpr uint32_t MK_MAX_SPLIT = 8;
 uint32_t merkle_split();
 
 // Split of a reduction level over `cur` hashes: the leaf level takes the split
-// as given; hash levels of at least 2^20 hashes (1024+ CTAs) take it too, smaller
-// ones reduce each tile to one root.
-inline uint32_t merkle_level_split(uint64_t cur, uint32_t split) { return cur >= (1ull << 20) ? split : 0u; }
+// as given; hash levels of at least 2^20 hashes (1024+ CTAs) take at most 5 (each
+// step then reduces 32-fold, so the chain stays short), smaller ones reduce each
+// tile to one root.
+inline uint32_t merkle_level_split(uint64_t cur, uint32_t split) {
+  return cur >= (1ull << 20) ? std::min<uint32_t>(split, 5) : 0u;
+}
 
 // Words of scratch merkle_root needs for n_leaves leaves with split `split` (0 when
 // n_leaves <= 1024): the sum of the hash levels it writes, in the order it writes
