@@ -151,7 +151,32 @@ def cpu_sample(args, threads: int):
                       f"{secs:.2f} s on {threads} threads"}
 
 
+def cpu_proofs(threads: int, n_proofs: int = 4, log_n: int = 16):
+    """Config 0 on the host: full Fibonacci prove + verify at log_n = 16 (a0 = 1, a1
+    seeded), the oracle's prover on `threads` threads (the reference's equivalent
+    is prove_lean, timed by src/bin/full_benchmark.rs:30-59)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as O
+    from vortexstark_b200.workloads import SplitMix64
+    g = SplitMix64(0x56530000)
+    jobs = [(1, g.m31()) for _ in range(n_proofs)]
+    O.prove(1, 1, log_n, threads=threads)  # warm-up
+    t0 = time.perf_counter()
+    ok = True
+    for a, b in jobs:
+        rc, _ = O.verify(O.prove(a, b, log_n, threads=threads))
+        ok = ok and rc == 0
+    secs = time.perf_counter() - t0
+    return {"value": n_proofs / secs, "unit": "proofs/s (prove + verify)", "cores": threads, "kind": "port",
+            "verified": ok, "sample": f"{n_proofs} Fibonacci proofs, log_n={log_n}, a0=1, a1 seeded; "
+                                      f"{secs:.2f} s on {threads} threads"}
+
+
 def run_reference(args):
+    """The CPU implementation of the path (the oracle port: the reference has no CPU
+    path for it) on the host cores, one bounded sample of the workload per step:
+    34 columns x 2^cpu_log_n rows, x4 LDE + row-packed root, and FRI of 2^(cpu_log_n+2).
+    ms_per_step is the sample's own measured time."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -161,14 +186,25 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_sample(args, threads)
-    vals = [cpu_sample(args, threads) for _ in range(args.steps)]
+    vals, secs = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        vals.append(cpu_sample(args, threads))
+        secs.append(time.perf_counter() - t0)
     v = statistics.mean(x["value"] for x in vals)
-    _, _, _, _, _, committed = workload(args)
+    n_cols, _, blow, _, _, committed = workload(args)
+    s_log = args.cpu_log_n
+    sample_elems = n_cols * (1 << (s_log + blow)) + 4 * ((1 << (s_log + blow)) - 8)
+    cfg = dict(config_json(args), sample=f"{n_cols} cols x 2^{s_log} rows (LDE 2^{s_log + blow}) + FRI of "
+                                         f"2^{s_log + blow} QM31 per step ({sample_elems} committed elements)",
+               sample_log_n=s_log)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": committed / v * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(secs) * 1e3,
+            "ms_per_step_full_config_derived": committed / v * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31)",
-            "data": "synthetic (seeded SplitMix64 uniform M31)", "config": config_json(args),
+            "data": "synthetic (seeded SplitMix64 uniform M31)", "config": cfg,
             "cpu_baseline": dict(vals[-1], value=v),
+            "cpu_proofs": cpu_proofs(threads),
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -393,33 +429,43 @@ def proof_workloads(args):
                     "proofs_per_s": len(plain) / t_plain, "p50_ms": W.percentile(lat, 0.5),
                     "p99_ms": W.percentile(lat, 0.99), "verified": ok}
     # Batches are throughput work: every job at the same stream priority (the
-    # size-priority default is the serving policy, measured below).
-    with api.Engine(args.slots, size_priority=False) as eng:
-        prep(eng, plain)
-        W.run_list(eng, plain[:16], sequential=False)
-        t_e, r_e = W.run_list(eng, plain, sequential=False)
+    # size-priority default is the serving policy, measured below). The engine
+    # proves queued Fibonacci jobs of one size as one batch (one graph launch, one
+    # kernel per stage for all of them); batch_limit 1 is one proof per launch.
+    def batched(jobs, limit, warm):
+        with api.Engine(args.slots, size_priority=False) as eng:
+            eng.set_batch_limit(limit)
+            prep(eng, jobs)
+            W.run_list(eng, jobs[:warm], sequential=False)
+            return W.run_list(eng, jobs, sequential=False)
+
+    t_e, r_e = batched(plain, 0, len(plain))
+    t_1, r_1 = batched(plain, 1, 16)
     out["batched_fib16"] = {"workload": "the same 64 proofs submitted at once to the slot engine",
                             "slots": args.slots, "proofs_per_s": len(plain) / t_e,
                             "vs_plain": t_plain / t_e,
-                            "identical_to_plain": all(x[0] == y for x, y in zip(r_e, r_plain))}
+                            "one_proof_per_launch_proofs_per_s": len(plain) / t_1,
+                            "identical_to_plain": all(x[0] == y for x, y in zip(r_e, r_plain)) and
+                            all(x[0] == y for x, y in zip(r_1, r_plain))}
 
     jobs = W.batched_jobs(64)
     W.run_plain(W.shapes(jobs))
     t_p, r_p = W.run_plain(jobs)
     with api.Engine(1, size_priority=False) as one:
+        one.set_batch_limit(1)
         prep(one, jobs)
         t_one, r_one = W.run_list(one, jobs, sequential=True)
-    with api.Engine(args.slots, size_priority=False) as eng:
-        prep(eng, jobs)
-        W.run_list(eng, jobs[:8], sequential=False)
-        t_b, r_b = W.run_list(eng, jobs, sequential=False)
+    t_b, r_b = batched(jobs, 0, len(jobs))
+    t_b1, r_b1 = batched(jobs, 1, 8)
     n_fib = sum(1 for j in jobs if j.kind == api.FIB)
     out["batched_mix"] = {
         "workload": "64 jobs, log_n U{16..22}: Fibonacci proofs (a1 seeded) or 1-34 seeded uniform columns (commit)",
         "slots": args.slots, "jobs_per_s": len(jobs) / t_b, "proofs_per_s": n_fib / t_b,
         "plain_path_jobs_per_s": len(jobs) / t_p, "engine_one_slot_jobs_per_s": len(jobs) / t_one,
+        "one_proof_per_launch_jobs_per_s": len(jobs) / t_b1,
         "vs_plain": t_p / t_b, "vs_one_slot": t_one / t_b,
-        "identical_plain_one_slot_batched": all(a == b[0] == c[0] for a, b, c in zip(r_p, r_one, r_b))}
+        "identical_plain_one_slot_batched": all(a == b[0] == c[0] == d[0] for a, b, c, d in zip(r_p, r_one, r_b, r_b1)),
+        "parity": mix_parity(jobs, r_p)}
 
     # Single-proof latency at the sizes the reference publishes (prove_lean(1, 1, log_n)
     # after a warm-up proof): the drop-in path and the graph-captured prover.
@@ -449,6 +495,43 @@ def proof_workloads(args):
                         "and 34-col commits 18/20/22", slots=args.slots, hbm_budget_gb=150,
                         stream_priority="by job size, smallest first" if by_size else "equal for all jobs")
     return out
+
+
+# ---------------------------------------------------------------- parity of the timed step
+def step_parity(args, rank, world, root, roots, last):
+    """The last timed step's row-packed root, FRI layer roots and last layer against
+    the oracle's results for the same seeded inputs (tests/golden/bench_digests.json,
+    written by tests/golden/gen_bench_digests.py). A mismatch stops the run: no
+    number is reported for wrong results."""
+    import numpy as np
+    path = ROOT / "tests" / "golden" / "bench_digests.json"
+    d = json.loads(path.read_text()).get("step") if path.exists() else None
+    same_cfg = d is not None and (d["n_cols"], d["log_n"], d["fri_log_n"]) == (args.cols, args.log_n, args.fri_log)
+    if not same_cfg or rank != 0:
+        return {"status": "unchecked", "why": "no oracle digest for this configuration" if not same_cfg
+                else "checked on rank 0 only"}
+    hexw = lambda t: t.cpu().numpy().view(np.uint32).tobytes().hex()  # noqa: E731
+    got_roots = [hexw(roots[8 * i:8 * i + 8]) for i in range(args.fri_log - 3)]
+    ok = hexw(root) == d["root"] and got_roots == d["fri_roots"] and hexw(last) == d["last_layer"]
+    if not ok:
+        raise SystemExit(f"bench: the timed step's results differ from the oracle digests in {path.name}")
+    return {"status": "digest-match", "checked": f"row-packed root, {args.fri_log - 3} FRI layer roots, last layer",
+            "oracle": "tests/golden/bench_digests.json"}
+
+
+def mix_parity(jobs, results):
+    """Results of the 64-job mix against the oracle's (bench_digests.json)."""
+    import hashlib
+    path = ROOT / "tests" / "golden" / "bench_digests.json"
+    exp = json.loads(path.read_text()).get("batched_mix", {}).get("results") if path.exists() else None
+    if not exp or len(exp) != len(jobs):
+        return "unchecked"
+    for e, r in zip(exp, results):
+        good = (len(r) == e["len"] and hashlib.sha256(r).hexdigest() == e["sha256"]) if e["kind"] == "fib" \
+            else r.hex() == e["root"]
+        if not good:
+            return "MISMATCH"
+    return "digest-match"
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -568,6 +651,7 @@ def main():
         torch.cuda.synchronize()
     launches = (api.launch_count() - l0) // args.steps
     ms = t0.elapsed_time(t1) / args.steps
+    parity = step_parity(args, rank, world, root, roots, last)
     phase = {"lde": 0.0, "merkle": 0.0, "fri": 0.0}
     for m in marks:
         phase["lde"] += m[0].elapsed_time(m[1]) / args.steps
@@ -690,11 +774,14 @@ def main():
         if not args.no_proofs:
             proofs = proof_workloads(args)
     if rank == 0:
-        cpu = None if args.no_cpu else cpu_sample(args, os.cpu_count() or 1)
+        cpu = None
+        if not args.no_cpu:
+            cpu = cpu_sample(args, os.cpu_count() or 1)
+            cpu["proofs"] = cpu_proofs(os.cpu_count() or 1)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic (seeded SplitMix64 uniform M31)",
-                "config": config_json(args), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "config": config_json(args), "parity": parity, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clk.summary(), "three_tree_commit": three, "oods": oods, "fri_fold_dropins": folds, "ntt_autotune": tuning,
                 "cairo": cairo, "proofs": proofs}
         print(json.dumps(line), flush=True)

@@ -271,9 +271,10 @@ int vs_merkle_root_rowpacked(const uint32_t* d_cols, uint64_t stride, uint32_t n
  * at that point (a server whose HBM is fully reserved by its admission budget, a
  * framework whose allocator owns device memory, a step that must not risk an
  * allocation failure or sync). No counterpart in the reference. Accepts at most
- * 2^26 leaves (VS_ERR_INVALID beyond). The first call on a device looks up the
- * array's device address; make it before any stream capture. All calls share the
- * array: calls whose work overlaps on the GPU race. */
+ * 2^26 leaves (VS_ERR_INVALID beyond). The first call on a device, and the first
+ * after the device's context was recreated, looks up the array's device address;
+ * make it before any stream capture. All calls share the array: calls whose work
+ * overlaps on the GPU race. */
 int vs_merkle_root_rowpacked_noalloc(const uint32_t* d_cols, uint64_t stride, uint32_t n_cols, uint32_t log_leaves,
                                      uint32_t* d_root, vs_stream_t stream);
 /* Merkle root with the reference's <=16-column leaf (blake2s.cu leaf semantics). */
@@ -316,13 +317,21 @@ int vs_prover_create(uint32_t log_n, void** prover);
 int vs_prover_prove(void* prover, uint32_t a, uint32_t b, uint8_t* h_out, uint64_t cap, uint64_t* out_len);
 int vs_prover_destroy(void* prover);
 
-/* Batched / served execution. An engine owns n_slots workers (host thread +
- * CUDA stream + cached per-shape workspaces). Submitted jobs queue in FIFO order;
- * a free slot starts the head job when the working sets of the running jobs plus
- * the head job fit hbm_budget_bytes (0 = unlimited; a job larger than the budget
- * runs alone). Results: a KRAK proof for VS_JOB_FIB, the 32-byte row-packed root
- * of the seeded columns' x4 stwo LDE for VS_JOB_COMMIT. Times are seconds since
- * engine creation. */
+/* Batched / served execution (no reference counterpart: the reference proves a
+ * batch one proof after another, ProverPipeline::prove_batch, src/prover.rs:2265-2270).
+ * An engine owns n_slots workers (host thread + CUDA streams) and a pool of cached
+ * device workspaces (batched provers, graph-captured provers, commitment buffers).
+ * Submitted jobs queue in FIFO order; a free slot takes the head job together with
+ * the queued Fibonacci jobs of the same trace size (log_n <= 22), up to that size's
+ * batch capacity, and proves them as one batch (one CUDA graph launch, one kernel
+ * per stage for all of them). A job runs when a cached workspace of its shape is
+ * idle or a new one keeps the engine's device memory (every cached workspace plus
+ * the library's twiddle tables) within hbm_budget_bytes (0 = unlimited); idle
+ * workspaces of other shapes are freed, least recently used first, to make room.
+ * A job whose workspace does not fit the budget even on an idle engine fails with
+ * VS_ERR_BUDGET. Results: a KRAK proof for VS_JOB_FIB, the 32-byte row-packed root
+ * of the seeded columns' x4 stwo LDE for VS_JOB_COMMIT; each result depends only
+ * on its job. Times are seconds since engine creation. */
 enum { VS_JOB_FIB = 0, VS_JOB_COMMIT = 1 };
 typedef struct {
   uint32_t kind;   /* VS_JOB_FIB or VS_JOB_COMMIT */
@@ -354,8 +363,37 @@ int vs_engine_submit(void* engine, const vs_job* job, uint64_t* ticket);
  * filled (the bytes stay available); otherwise the bytes are copied and the
  * ticket is retired. */
 int vs_engine_wait(void* engine, uint64_t ticket, vs_job_result* result, uint8_t* h_out, uint64_t cap);
+/* As vs_engine_wait, giving up after timeout_s seconds (negative: no limit) with
+ * VS_ERR_TIMEOUT; the ticket stays valid. A failed, cancelled or rejected job
+ * returns its status (VS_ERR_CANCELLED, VS_ERR_BUDGET, VS_ERR_OOM, ...); with
+ * h_out != NULL its ticket is retired. */
+int vs_engine_wait_for(void* engine, uint64_t ticket, double timeout_s, vs_job_result* result, uint8_t* h_out,
+                       uint64_t cap);
+/* Cancels a job that has not started: VS_OK, and its wait returns
+ * VS_ERR_CANCELLED. A running or finished job cannot be cancelled (VS_ERR_BUSY). */
+int vs_engine_cancel(void* engine, uint64_t ticket);
 int vs_engine_drain(void* engine);
 double vs_engine_now(void* engine);
+/* At most max_jobs proofs per batch (0 = each size's default capacity, 1 = one
+ * proof per graph launch). Takes effect for workspaces created afterwards. */
+int vs_engine_set_batch_limit(void* engine, uint32_t max_jobs);
+/* Device bytes of the workspace a job of this shape runs in (a batch workspace
+ * for small Fibonacci proofs), not counting twiddle tables. */
+int vs_engine_workspace_bytes(void* engine, const vs_job* shape, uint64_t* bytes);
+/* Host-side fault injection for tests: the next `count` workspace creations fail
+ * with VS_ERR_OOM before allocating anything; the engine stays usable. */
+int vs_engine_inject_alloc_failures(void* engine, uint32_t count);
+typedef struct {
+  uint64_t budget_bytes;        /* 0: unlimited */
+  uint64_t resident_bytes;      /* cached workspaces, idle and in use */
+  uint64_t twiddle_bytes;       /* the library's twiddle tables on the engine's device */
+  uint64_t peak_held_bytes;     /* largest resident + twiddle bytes admitted so far */
+  uint64_t evictions;           /* idle workspaces freed to make room */
+  uint64_t workspaces_created;
+  uint32_t idle_workspaces, busy_workspaces;
+  uint32_t queued, running;     /* jobs */
+} vs_engine_stats;
+int vs_engine_get_stats(void* engine, vs_engine_stats* out);
 
 /* Release cached twiddles and scratch of the current device. */
 int vs_release_caches(void);

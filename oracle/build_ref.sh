@@ -3,14 +3,15 @@
 # reference sources, into oracle/_ref/libvortex_ref.so. Test infrastructure only: the
 # GPU parity tests use it to pin the CPU oracle against the reference's kernels, and
 # tests/golden/gen_ref_golden.py uses it to produce the committed golden vectors.
-# Needs the reference checkout (REF_ROOT, default /root/reference); on a machine without
-# it the prebuilt library is used as is.
+# Needs the path of the reference checkout, as the first argument or in REF_ROOT;
+# without it (or on a machine without the checkout) the prebuilt library is kept.
+#     oracle/build_ref.sh <reference checkout>
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF_ROOT="${REF_ROOT:-/root/reference}"
+REF_ROOT="${1:-${REF_ROOT:-}}"
 OUT="$HERE/_ref"
-if [ ! -d "$REF_ROOT/cuda" ]; then
-  echo "reference sources not found at $REF_ROOT; keeping prebuilt $OUT" >&2
+if [ -z "$REF_ROOT" ] || [ ! -d "$REF_ROOT/cuda" ]; then
+  echo "reference sources not given or not found (REF_ROOT='$REF_ROOT'); keeping prebuilt $OUT" >&2
   exit 0
 fi
 mkdir -p "$OUT"

@@ -107,14 +107,32 @@ def test_engine_mix_equals_alone_and_oracle(L):
 
 
 def test_engine_budget_admission(L):
-    """A budget below two jobs' working sets serialises them; results are unchanged."""
-    jobs = [Job(0, 10, 1, 2, 0, 0, 0), Job(0, 10, 3, 4, 0, 0, 0), Job(1, 9, 0, 0, 20, 0, 77)]
-    res = run_engine(L, jobs, slots=3, budget=1 << 20)
-    assert res[0][0] == O.prove(1, 2, 10) and res[1][0] == O.prove(3, 4, 10)
-    assert res[2][0] == commit_root_oracle(9, 20, 77)
+    """A budget that holds one workspace at a time serialises jobs of different
+    shapes (the idle workspace of one shape is freed for the next); results are
+    unchanged."""
+    from vortexstark_b200 import api
+    jobs = [api.fib_job(10, 1, 2), api.commit_job(9, 20, 77), api.fib_job(11, 3, 4)]
+    with api.Engine(1) as probe:
+        biggest = max(probe.workspace_bytes(j) for j in jobs)
+    tw = api_twiddle_margin()
+    with api.Engine(3, biggest + tw) as eng:
+        tickets = [eng.submit(j) for j in jobs]
+        res = [eng.wait(t) for t in tickets]
+        st = eng.stats()
+    assert res[0][0] == O.prove(1, 2, 10) and res[2][0] == O.prove(3, 4, 11)
+    assert res[1][0] == commit_root_oracle(9, 20, 77)
     spans = sorted((r[2], r[3]) for r in res)
     for (s0, e0), (s1, e1) in zip(spans, spans[1:]):
         assert s1 >= e0 - 1e-6  # no two ran at the same time
+    assert st["peak_held_bytes"] <= biggest + tw and st["evictions"] >= 2
+
+
+def api_twiddle_margin():
+    """Budget margin covering the twiddle tables the engine counts (cached ones of
+    earlier tests included) plus the tables small test shapes build."""
+    from vortexstark_b200 import api
+    with api.Engine(1) as e:
+        return e.stats()["twiddle_bytes"] + (64 << 20)
 
 
 def test_engine_rejects_bad_jobs(L):
@@ -138,3 +156,158 @@ def test_engine_priority_policy_does_not_change_results(L):
     assert [r[0] for r in by_size] == [r[0] for r in fifo]
     eng = C.c_void_p()
     assert L.vs_engine_create_ex(2, 0, 0x80, C.byref(eng)) == 1  # unknown flag rejected
+
+
+# ---------------------------------------------------------------- batched proofs, budget, failure paths
+def _occupy_then_submit(eng, jobs, log_n_block=18):
+    """Submits a blocking commitment first, so the following jobs queue up and a
+    slot takes them as one batch."""
+    from vortexstark_b200 import api
+    first = eng.submit(api.commit_job(log_n_block, 34, 0x77))
+    return first, [eng.submit(j) for j in jobs]
+
+
+@pytest.mark.parametrize("log_n", [4, 7, 10, 13])
+def test_batched_proofs_match_oracle_and_plain(L, log_n):
+    """Jobs of one size queued together run as one batch (one graph launch); every
+    proof equals the oracle's, vs_prove_fib's and the unbatched engine's bytes."""
+    from vortexstark_b200 import api
+    pairs = [(1, 1), (1, 5), (3, 4), (7, 123456789), (2**31 - 2, 0), (0, 0)]
+    jobs = [api.fib_job(log_n, a, b) for a, b in pairs]
+    with api.Engine(1) as eng:
+        first, ts = _occupy_then_submit(eng, jobs)
+        eng.wait(first)
+        batched = [eng.wait(t) for t in ts]
+    # all but possibly the first job started together: one batch
+    assert len({round(r[2], 9) for r in batched[1:]}) == 1
+    with api.Engine(2) as eng:
+        eng.set_batch_limit(1)
+        single = [eng.wait(eng.submit(j))[0] for j in jobs]
+    for (a, b), r, s1 in zip(pairs, batched, single):
+        assert r[0] == s1 == O.prove(a, b, log_n) == api.prove_fib(a, b, log_n)
+    assert api.verify_fib(batched[0][0]) == (True, "")
+
+
+def test_batch_capacity_limit_and_mixed_sizes(L):
+    """Batches never mix sizes or exceed the limit; results do not depend on batching."""
+    from vortexstark_b200 import api
+    rng = np.random.default_rng(11)
+    jobs = [api.fib_job(int(rng.integers(5, 9)), 1, int(rng.integers(0, 2**31 - 1))) for _ in range(20)]
+    with api.Engine(2) as eng:
+        eng.set_batch_limit(3)
+        first, ts = _occupy_then_submit(eng, jobs)
+        eng.wait(first)
+        res = [eng.wait(t) for t in ts]
+    starts = {}
+    for j, r in zip(jobs, res):
+        starts.setdefault(round(r[2], 9), set()).add(j.log_n)
+    assert all(len(v) == 1 for v in starts.values())  # one size per batch
+    counts = {}
+    for r in res:
+        counts[round(r[2], 9)] = counts.get(round(r[2], 9), 0) + 1
+    assert max(counts.values()) <= 3
+    for j, r in zip(jobs, res):
+        assert r[0] == O.prove(j.a, j.b, j.log_n)
+
+
+def test_engine_holds_at_most_the_budget(L):
+    """With a budget below the sum of the shapes' workspaces the engine frees idle
+    workspaces to admit new shapes: its accounted peak and the device memory it
+    actually takes (cudaMemGetInfo) stay within the budget, and results match an
+    unlimited engine."""
+    import threading
+    import time
+
+    from vortexstark_b200 import api
+    shapes = [api.fib_job(15, 1, 0), api.fib_job(16, 1, 0), api.commit_job(17, 20, 0), api.commit_job(16, 34, 0),
+              api.fib_job(17, 1, 0)]
+    rng = np.random.default_rng(3)
+    jobs = []
+    for i in range(24):
+        s = shapes[int(rng.integers(0, len(shapes)))]
+        if s.kind == api.FIB:
+            jobs.append(api.fib_job(s.log_n, 1, int(rng.integers(0, 2**31 - 1))))
+        else:
+            jobs.append(api.commit_job(s.log_n, s.n_cols, int(rng.integers(1, 1 << 40))))
+    with api.Engine(1) as probe:
+        probe.set_batch_limit(4)
+        sizes = [probe.workspace_bytes(s) for s in shapes]
+    with api.Engine(1) as e:
+        tw_now = e.stats()["twiddle_bytes"]
+    budget = max(sizes) * 2 + tw_now + (32 << 20)  # + the twiddle tables these shapes build
+    assert budget < sum(sizes) * 2  # not every shape (two slots' worth) fits at once
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    low = [free0]
+    stop = False
+
+    def poll():
+        while not stop:
+            low[0] = min(low[0], torch.cuda.mem_get_info()[0])
+            time.sleep(0.002)
+
+    th = threading.Thread(target=poll)
+    th.start()
+    try:
+        with api.Engine(2, budget, size_priority=False) as eng:
+            eng.set_batch_limit(4)
+            ts = [eng.submit(j) for j in jobs]
+            got = [eng.wait(t)[0] for t in ts]
+            st = eng.stats()
+    finally:
+        stop = True
+        th.join()
+    assert st["peak_held_bytes"] <= budget
+    assert st["evictions"] > 0
+    assert free0 - low[0] <= budget + (64 << 20)  # context-side graph/stream memory as slack
+    with api.Engine(2) as eng:
+        eng.set_batch_limit(4)
+        ref = [eng.wait(eng.submit(j))[0] for j in jobs]
+    assert got == ref
+
+
+def test_engine_rejects_job_above_budget(L):
+    from vortexstark_b200 import api
+    with api.Engine(2, 1 << 20) as eng:
+        rc, out = eng.wait_status(eng.submit(api.fib_job(10, 1, 1)))
+        assert rc == api.VS_ERR_BUDGET and out == b""
+        assert eng.stats()["resident_bytes"] == 0
+
+
+def test_engine_cancel_and_timeout(L):
+    """A queued job can be cancelled; a bounded wait on a running job times out
+    (the ticket stays valid) and the job still completes."""
+    import time
+
+    from vortexstark_b200 import api
+    with api.Engine(1) as eng:
+        eng.prepare(api.fib_job(22, 1, 1))
+        long_t = eng.submit(api.fib_job(22, 1, 1))
+        t0 = time.time()
+        while eng.stats()["running"] == 0 and time.time() - t0 < 10:
+            time.sleep(0.0001)
+        queued = [eng.submit(api.fib_job(8, 1, k)) for k in range(3)]
+        assert eng.cancel(queued[1]) == 0
+        r = JobResult()
+        rc = L.vs_engine_wait_for(eng.h, long_t, 0.0, C.byref(r), None, 0)  # length query: nothing retired
+        assert rc in (0, api.VS_ERR_TIMEOUT)
+        assert eng.cancel(long_t) == api.VS_ERR_BUSY  # running or finished: not cancellable
+        assert eng.wait(long_t)[0] == api.prove_fib(1, 1, 22)
+        assert eng.wait_status(queued[1])[0] == api.VS_ERR_CANCELLED
+        assert eng.wait(queued[0])[0] == O.prove(1, 0, 8)
+        assert eng.wait(queued[2])[0] == O.prove(1, 2, 8)
+        assert L.vs_engine_cancel(eng.h, 10**9) == 1  # unknown ticket
+
+
+def test_engine_injected_allocation_failure(L):
+    """A workspace allocation that fails (injected on the host) fails its job with
+    VS_ERR_OOM and leaves the engine usable, with nothing counted as resident."""
+    from vortexstark_b200 import api
+    with api.Engine(1) as eng:
+        eng.inject_alloc_failures(1)
+        rc, _ = eng.wait_status(eng.submit(api.fib_job(9, 1, 3)))
+        assert rc == api.VS_ERR_OOM
+        assert eng.stats()["resident_bytes"] == 0
+        assert eng.wait(eng.submit(api.fib_job(9, 1, 3)))[0] == O.prove(1, 3, 9)
+        st = eng.stats()
+        assert st["resident_bytes"] > 0 and st["idle_workspaces"] == 1

@@ -199,7 +199,16 @@ class JobResult(C.Structure):
                 ("t_start", C.c_double), ("t_end", C.c_double)]
 
 
+class EngineStats(C.Structure):
+    """Mirror of vs_engine_stats (include/vstark.h)."""
+    _fields_ = [("budget_bytes", C.c_uint64), ("resident_bytes", C.c_uint64), ("twiddle_bytes", C.c_uint64),
+                ("peak_held_bytes", C.c_uint64), ("evictions", C.c_uint64), ("workspaces_created", C.c_uint64),
+                ("idle_workspaces", C.c_uint32), ("busy_workspaces", C.c_uint32), ("queued", C.c_uint32),
+                ("running", C.c_uint32)]
+
+
 FIB, COMMIT = 0, 1
+VS_ERR_BUDGET, VS_ERR_TIMEOUT, VS_ERR_CANCELLED, VS_ERR_BUSY, VS_ERR_OOM = 4, 5, 6, 7, 3
 
 
 def fib_job(log_n: int, a: int, b: int) -> Job:
@@ -228,11 +237,42 @@ class Engine:
         check(lib().vs_engine_submit(self.h, C.byref(job), C.byref(t)), "vs_engine_submit")
         return t.value
 
-    def wait(self, ticket: int):
-        """Returns (result bytes, t_submit, t_start, t_end) in engine seconds."""
+    def wait(self, ticket: int, timeout_s: float | None = None):
+        """Returns (result bytes, t_submit, t_start, t_end) in engine seconds. With a
+        timeout, raises VstarkError (status VS_ERR_TIMEOUT = 5) when the job is not
+        done in time; the ticket stays valid."""
         r = JobResult()
-        check(lib().vs_engine_wait(self.h, ticket, C.byref(r), self._buf, PROOF_CAP), "vs_engine_wait")
+        t = -1.0 if timeout_s is None else float(timeout_s)
+        check(lib().vs_engine_wait_for(self.h, ticket, t, C.byref(r), self._buf, PROOF_CAP), "vs_engine_wait")
         return C.string_at(self._buf, r.out_len), r.t_submit, r.t_start, r.t_end
+
+    def wait_status(self, ticket: int, timeout_s: float | None = None) -> tuple[int, bytes]:
+        """(status, result bytes) without raising; status 0 = done."""
+        r = JobResult()
+        t = -1.0 if timeout_s is None else float(timeout_s)
+        rc = lib().vs_engine_wait_for(self.h, ticket, t, C.byref(r), self._buf, PROOF_CAP)
+        return rc, (C.string_at(self._buf, r.out_len) if rc == 0 else b"")
+
+    def cancel(self, ticket: int) -> int:
+        """0 when the queued job was cancelled; VS_ERR_BUSY (7) when it already runs or ran."""
+        return int(lib().vs_engine_cancel(self.h, ticket))
+
+    def set_batch_limit(self, max_jobs: int) -> None:
+        """At most max_jobs proofs per batched graph launch (0: per-size default, 1: no batching)."""
+        check(lib().vs_engine_set_batch_limit(self.h, max_jobs), "vs_engine_set_batch_limit")
+
+    def workspace_bytes(self, job: Job) -> int:
+        b = C.c_uint64()
+        check(lib().vs_engine_workspace_bytes(self.h, C.byref(job), C.byref(b)), "vs_engine_workspace_bytes")
+        return b.value
+
+    def inject_alloc_failures(self, count: int) -> None:
+        check(lib().vs_engine_inject_alloc_failures(self.h, count), "vs_engine_inject_alloc_failures")
+
+    def stats(self) -> dict:
+        st = EngineStats()
+        check(lib().vs_engine_get_stats(self.h, C.byref(st)), "vs_engine_get_stats")
+        return {f: getattr(st, f) for f, _ in EngineStats._fields_}
 
     def drain(self) -> None:
         lib().vs_engine_drain(self.h)

@@ -84,7 +84,8 @@ struct LeafFoldD {
 // ------------------------------------------------------------------ device stages
 __global__ void fib_trace_params_kernel(const uint32_t* __restrict__ ab, uint32_t* __restrict__ out, uint64_t n) {
   __shared__ uint32_t sm[256 * 33];
-  const uint32_t a = ab[0], b = ab[1];
+  const uint32_t a = ab[2 * blockIdx.y], b = ab[2 * blockIdx.y + 1];
+  out += (uint64_t)blockIdx.y * n;
   const uint64_t base = (uint64_t)blockIdx.x * 256 * 32;
   const uint64_t s = base + (uint64_t)threadIdx.x * 32;
   uint32_t m00 = 1, m01 = 0, m11 = 1, b00 = 1, b01 = 1, b11 = 0;
@@ -226,6 +227,61 @@ __global__ void __launch_bounds__(256) paths_kernel(Leaf leaf, uint32_t TL, uint
   }
 }
 
+// ------------------------------------------------------------------ proof arena (shared with batch_prover.cu)
+void ArenaLayout::plan(uint32_t ln) {
+  log_n = ln;
+  log_eval = ln + BLOWUP_BITS;
+  nf = log_eval - LOG_LAST_LAYER;
+  tree.clear();
+  depth.clear();
+  size_t w = 0;
+  roots = w; w += 8 * (2 + nf);
+  last = w; w += 32;
+  q = w; w += N_QUERIES;
+  tv = w; w += 2 * N_QUERIES;
+  qv = w; w += 2 * N_QUERIES * 4;
+  fv = w; w += (size_t)nf * 2 * N_QUERIES * 4;
+  depth.push_back(log_eval);
+  depth.push_back(log_eval);
+  for (uint32_t l = 0; l < nf; l++) depth.push_back(log_eval - 1 - l);
+  for (uint32_t d : depth) { tree.push_back(w); w += (size_t)2 * N_QUERIES * d * 8; }
+  words = w;
+}
+
+// KRAK v1 from a host copy of the arena (after the stream completed).
+void ArenaLayout::serialize(const uint32_t* A, uint32_t a, uint32_t b, std::vector<uint8_t>& w) const {
+  auto w32 = [&](uint32_t v) { for (int k = 0; k < 4; k++) w.push_back((uint8_t)(v >> (8 * k))); };
+  auto wn = [&](const uint32_t* p, size_t cnt) { for (size_t i = 0; i < cnt; i++) w32(p[i]); };
+  auto wpaths = [&](size_t off, uint32_t d, uint32_t s) {
+    for (uint32_t qi = 0; qi < N_QUERIES; qi++) { w32(d); wn(A + off + ((size_t)(s * N_QUERIES + qi) * d) * 8, (size_t)d * 8); }
+  };
+  w.clear();
+  w.reserve(words * 4 + 4096);
+  w32(0x4B52414Bu); w32(1); w32(log_n); w32(a); w32(b);
+  wn(A + roots, 16);
+  w32(nf);
+  wn(A + roots + 16, 8 * nf);
+  w32(8);
+  wn(A + last, 32);
+  w32(N_QUERIES);
+  wn(A + q, N_QUERIES);
+  w32(N_QUERIES);
+  wn(A + tv, 2 * N_QUERIES);
+  wpaths(tree[0], depth[0], 0);
+  wpaths(tree[0], depth[0], 1);
+  w32(N_QUERIES);
+  wn(A + qv, 2 * N_QUERIES * 4);
+  wpaths(tree[1], depth[1], 0);
+  wpaths(tree[1], depth[1], 1);
+  w32(nf);
+  for (uint32_t l = 0; l < nf; l++) {
+    w32(N_QUERIES);
+    wn(A + fv + (size_t)l * 2 * N_QUERIES * 4, 2 * N_QUERIES * 4);
+    wpaths(tree[2 + l], depth[2 + l], 0);
+    wpaths(tree[2 + l], depth[2 + l], 1);
+  }
+}
+
 // ------------------------------------------------------------------ the prover
 struct TreeBufs {
   uint64_t n = 0;
@@ -241,6 +297,7 @@ struct GraphProver::Impl {
   cudaStream_t st = nullptr;
   cudaStream_t running = nullptr;  // stream of the proof in flight
   std::vector<void*> allocs;
+  uint64_t allocated = 0;  // device bytes of allocs
   uint32_t *d_ab = nullptr, *h_ab = nullptr, *d_trace = nullptr, *d_eval = nullptr, *d_alpha = nullptr,
            *d_qidx = nullptr, *d_arena = nullptr, *h_arena = nullptr;
   ChanDev* d_ch = nullptr;
@@ -249,10 +306,7 @@ struct GraphProver::Impl {
   std::vector<TreeBufs> fri_t;
   // subroot scratch shared by the trees (committed one after another in the graph)
   uint32_t split = 0, *sub_a = nullptr, *sub_b = nullptr;
-  // arena layout (words)
-  size_t a_roots = 0, a_last = 0, a_q = 0, a_tv = 0, a_qv = 0, a_fv = 0, a_paths = 0, words = 0;
-  std::vector<size_t> a_tree;  // path region per tree: trace, quot, fri...
-  std::vector<uint32_t> depth;
+  ArenaLayout lay;
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
 
@@ -269,8 +323,10 @@ struct GraphProver::Impl {
   template <class T>
   int alloc(T** p, uint64_t count) {
     void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, std::max<uint64_t>(count, 1) * sizeof(T));
+    const uint64_t bytes = std::max<uint64_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) return set_error(VS_ERR_OOM, "prover workspace: %s", cudaGetErrorString(e));
+    allocated += (bytes + 511) & ~511ull;  // cudaMalloc's granularity
     allocs.push_back(q);
     *p = (T*)q;
     return VS_OK;
@@ -341,22 +397,9 @@ struct GraphProver::Impl {
       fri_vals.push_back({base, base + half, base + 2 * half, base + 3 * half});
       VS_TRY(tree_bufs(fri_t[l], half));
     }
-    // arena
-    size_t w = 0;
-    a_roots = w; w += 8 * (2 + nf);
-    a_last = w; w += 32;
-    a_q = w; w += N_QUERIES;
-    a_tv = w; w += 2 * N_QUERIES;
-    a_qv = w; w += 2 * N_QUERIES * 4;
-    a_fv = w; w += (size_t)nf * 2 * N_QUERIES * 4;
-    a_paths = w;
-    depth.push_back(log_eval);
-    depth.push_back(log_eval);
-    for (uint32_t l = 0; l < nf; l++) depth.push_back(log_eval - 1 - l);
-    for (uint32_t d : depth) { a_tree.push_back(w); w += (size_t)2 * N_QUERIES * d * 8; }
-    words = w;
-    VS_TRY(alloc(&d_arena, words));
-    VS_CUDA(cudaMallocHost((void**)&h_arena, words * 4));
+    lay.plan(log_n);
+    VS_TRY(alloc(&d_arena, lay.words));
+    VS_CUDA(cudaMallocHost((void**)&h_arena, lay.words * 4));
     // twiddles and fold twiddles are built (and cached) outside the capture
     const TwiddleSet* tw = nullptr;
     VS_TRY(get_twiddles(TW_NATIVE, log_n, &tw, st));
@@ -385,11 +428,11 @@ struct GraphProver::Impl {
     VS_LAUNCHED("fib_trace_params_kernel");
     VS_TRY(lde_cached(TW_NATIVE, d_trace, 0, d_eval, 0, 1, log_n, BLOWUP_BITS, st));
     VS_TRY(commit(LeafOne{d_eval}, trace_t));
-    ch_mix_draw_kernel<<<1, 32, 0, st>>>(d_ch, 1, trace_t.layers.back(), d_arena + a_roots, d_alpha);
+    ch_mix_draw_kernel<<<1, 32, 0, st>>>(d_ch, 1, trace_t.layers.back(), d_arena + lay.roots, d_alpha);
     VS_LAUNCHED("ch_mix_draw_kernel");
     const LeafFibQuotD quot{d_eval, N - 1, d_alpha};
     VS_TRY(commit(quot, quot_t));
-    ch_mix_draw_kernel<<<1, 32, 0, st>>>(d_ch, 0, quot_t.layers.back(), d_arena + a_roots + 8, d_alpha + 4);
+    ch_mix_draw_kernel<<<1, 32, 0, st>>>(d_ch, 0, quot_t.layers.back(), d_arena + lay.roots + 8, d_alpha + 4);
     VS_LAUNCHED("ch_mix_draw_kernel");
     for (uint32_t l = 0; l < nf; l++) {
       const uint32_t cur = log_eval - l;
@@ -404,70 +447,36 @@ struct GraphProver::Impl {
                        {fri_vals[l][0], fri_vals[l][1], fri_vals[l][2], fri_vals[l][3]}, tw, a};
         VS_TRY(commit(leaf, fri_t[l]));
       }
-      ch_mix_draw_kernel<<<1, 32, 0, st>>>(d_ch, 0, fri_t[l].layers.back(), d_arena + a_roots + 8 * (2 + l),
+      ch_mix_draw_kernel<<<1, 32, 0, st>>>(d_ch, 0, fri_t[l].layers.back(), d_arena + lay.roots + 8 * (2 + l),
                                            l + 1 < nf ? d_alpha + 4 * (2 + l) : nullptr);
       VS_LAUNCHED("ch_mix_draw_kernel");
     }
     const auto& last = fri_vals[nf - 1];
-    ch_queries_kernel<<<1, 32, 0, st>>>(d_ch, last[0], last[1], last[2], last[3], d_arena + a_last, d_qidx,
-                                        d_arena + a_q, log_eval);
+    ch_queries_kernel<<<1, 32, 0, st>>>(d_ch, last[0], last[1], last[2], last[3], d_arena + lay.last, d_qidx,
+                                        d_arena + lay.q, log_eval);
     VS_LAUNCHED("ch_queries_kernel");
     DecParams dp{};
     dp.eval = d_eval;
     dp.mask = (uint32_t)(N - 1);
     dp.alpha = d_alpha;
     dp.qidx = d_qidx;
-    dp.trace_vals = d_arena + a_tv;
-    dp.quot_vals = d_arena + a_qv;
+    dp.trace_vals = d_arena + lay.tv;
+    dp.quot_vals = d_arena + lay.qv;
     dp.nf = nf;
     for (uint32_t l = 0; l < nf; l++)
       for (int k = 0; k < 4; k++) dp.fri[l][k] = fri_vals[l][k];
-    dp.fri_vals = d_arena + a_fv;
+    dp.fri_vals = d_arena + lay.fv;
     decommit_values_kernel<<<1, 2 * N_QUERIES, 0, st>>>(dp);
     VS_LAUNCHED("decommit_values_kernel");
-    VS_TRY(paths(LeafOne{d_eval}, trace_t, 0, a_tree[0]));
-    VS_TRY(paths(quot, quot_t, 0, a_tree[1]));
+    VS_TRY(paths(LeafOne{d_eval}, trace_t, 0, lay.tree[0]));
+    VS_TRY(paths(quot, quot_t, 0, lay.tree[1]));
     for (uint32_t l = 0; l < nf; l++)
       VS_TRY(paths(LeafSoa4{fri_vals[l][0], fri_vals[l][1], fri_vals[l][2], fri_vals[l][3]}, fri_t[l], l + 1,
-                   a_tree[2 + l]));
-    VS_CUDA(cudaMemcpyAsync(h_arena, d_arena, words * 4, cudaMemcpyDeviceToHost, st));
+                   lay.tree[2 + l]));
+    VS_CUDA(cudaMemcpyAsync(h_arena, d_arena, lay.words * 4, cudaMemcpyDeviceToHost, st));
     return VS_OK;
   }
 
-  // KRAK v1 from the host arena (after the stream completed).
-  void serialize(uint32_t a, uint32_t b, std::vector<uint8_t>& w) const {
-    const uint32_t* A = h_arena;
-    auto w32 = [&](uint32_t v) { for (int k = 0; k < 4; k++) w.push_back((uint8_t)(v >> (8 * k))); };
-    auto wn = [&](const uint32_t* p, size_t cnt) { for (size_t i = 0; i < cnt; i++) w32(p[i]); };
-    auto wpaths = [&](size_t off, uint32_t d, uint32_t s) {
-      for (uint32_t q = 0; q < N_QUERIES; q++) { w32(d); wn(A + off + ((size_t)(s * N_QUERIES + q) * d) * 8, (size_t)d * 8); }
-    };
-    w.clear();
-    w.reserve(words * 4 + 4096);
-    w32(0x4B52414Bu); w32(1); w32(log_n); w32(a); w32(b);
-    wn(A + a_roots, 16);
-    w32(nf);
-    wn(A + a_roots + 16, 8 * nf);
-    w32(8);
-    wn(A + a_last, 32);
-    w32(N_QUERIES);
-    wn(A + a_q, N_QUERIES);
-    w32(N_QUERIES);
-    wn(A + a_tv, 2 * N_QUERIES);
-    wpaths(a_tree[0], depth[0], 0);
-    wpaths(a_tree[0], depth[0], 1);
-    w32(N_QUERIES);
-    wn(A + a_qv, 2 * N_QUERIES * 4);
-    wpaths(a_tree[1], depth[1], 0);
-    wpaths(a_tree[1], depth[1], 1);
-    w32(nf);
-    for (uint32_t l = 0; l < nf; l++) {
-      w32(N_QUERIES);
-      wn(A + a_fv + (size_t)l * 2 * N_QUERIES * 4, 2 * N_QUERIES * 4);
-      wpaths(a_tree[2 + l], depth[2 + l], 0);
-      wpaths(a_tree[2 + l], depth[2 + l], 1);
-    }
-  }
 };
 
 GraphProver::GraphProver() : impl(new Impl) {}
@@ -479,12 +488,19 @@ int GraphProver::init(uint32_t log_n, int priority) {
 uint32_t GraphProver::log_n() const { return impl->log_n; }
 int GraphProver::device() const { return impl->device; }
 cudaStream_t GraphProver::stream() const { return impl->st; }
-uint64_t GraphProver::device_bytes() const {
-  uint64_t b = 0;
-  b += impl->n * 4 + impl->N * 4 * 3 + impl->words * 4;  // trace, eval, tile levels (<N/2 words each), arena
-  for (uint32_t l = 0; l < impl->nf; l++) b += (impl->N >> (l + 1)) * 16;
-  b += merkle_tile_scratch_bytes(impl->N, impl->split);
-  return b;
+uint64_t GraphProver::device_bytes() const { return impl->allocated; }
+
+// An upper bound of device_bytes() for a prover of 2^log_n rows, known before it
+// is created: trace, evaluation, arena and FRI layers as allocated, the tile-root
+// levels of all trees (under N/2 words together) and the allocation rounding
+// bounded by another 2N words, and subroot scratch at the largest tile split.
+uint64_t GraphProver::bytes_estimate(uint32_t log_n) {
+  ArenaLayout lay;
+  lay.plan(log_n);
+  const uint64_t n = 1ull << log_n, N = n << BLOWUP_BITS;
+  uint64_t b = n * 4 + N * 4 * 3 + lay.words * 4 + (64u << 10);
+  for (uint32_t l = 0; l < lay.nf; l++) b += (N >> (l + 1)) * 16;
+  return b + merkle_tile_scratch_bytes(N, MK_TILE_SPLIT_MAX);
 }
 int GraphProver::launch(uint32_t a, uint32_t b, cudaStream_t on) {
   if (a >= h::P || b >= h::P) return set_error(VS_ERR_INVALID, "public inputs must be canonical M31");
@@ -496,7 +512,8 @@ int GraphProver::launch(uint32_t a, uint32_t b, cudaStream_t on) {
 }
 int GraphProver::finish(uint32_t a, uint32_t b, std::vector<uint8_t>& out) {
   VS_CUDA(cudaStreamSynchronize(impl->running ? impl->running : impl->st));
-  impl->serialize(a, b, out);
+  impl->running = nullptr;  // the launch stream may be reused for other work from here on
+  impl->lay.serialize(impl->h_arena, a, b, out);
   return VS_OK;
 }
 bool GraphProver::busy() const {

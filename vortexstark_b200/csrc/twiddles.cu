@@ -224,6 +224,7 @@ int get_twiddles(int kind, uint32_t log_n, const TwiddleSet** out, cudaStream_t 
     const size_t lp = ((size_t)(n - 1) + 3) & ~(size_t)3, cp = ((size_t)(n / 2) + 3) & ~(size_t)3;
     size_t words = 2 * lp + 2 * cp;
     if (cudaMalloc(&t->mem, words * 4) != cudaSuccess) { delete t; return set_error(VS_ERR_OOM, "twiddles: alloc"); }
+    t->bytes = words * 4;
     t->line = t->mem;
     t->iline = t->line + lp;
     t->circle = t->iline + lp;
@@ -238,6 +239,7 @@ int get_twiddles(int kind, uint32_t log_n, const TwiddleSet** out, cudaStream_t 
   } else {
     HostCoset c = host_coset(COSET_HALF_ODDS, log_n - 1);
     if (cudaMalloc(&t->mem, (size_t)n * 4) != cudaSuccess) { delete t; return set_error(VS_ERR_OOM, "twiddles: alloc"); }
+    t->bytes = (uint64_t)n * 4;
     t->line = t->mem;
     t->iline = t->mem + n / 2;
     stwo_table_kernel<<<blocks_for(n / 2, th), th, 0, st>>>(c.initial, c.step, log_n, t->line);
@@ -263,6 +265,7 @@ int get_fold_twiddles(int which, uint32_t log_n, const uint32_t** out, cudaStrea
   t->log_n = log_n;
   const uint32_t half = 1u << (log_n - 1);
   if (cudaMalloc(&t->mem, (size_t)half * 2 * 4) != cudaSuccess) { delete t; return set_error(VS_ERR_OOM, "fold twiddles: alloc"); }
+  t->bytes = (uint64_t)half * 2 * 4;
   HostCoset c = host_coset(which == FOLD_CANONIC_CIRCLE ? COSET_HALF_COSET : which, log_n);
   // half_odds(L-1) has half_coset(L)'s initial point and twice its step; with the
   // L-bit reversal of 2i this gives half_odds(L-1).at(brev_{L-1}(i)).
@@ -277,6 +280,25 @@ int get_fold_twiddles(int which, uint32_t log_n, const uint32_t** out, cudaStrea
   g_cache[key(dev, kind, log_n)] = t;
   *out = t->line;
   return VS_OK;
+}
+
+uint64_t twiddle_bytes_if_missing(int device, int kind, uint32_t log_n) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_cache.count(key(device, kind, log_n))) return 0;
+  const uint64_t n = 1ull << log_n;
+  if (kind == TW_NATIVE) {
+    const uint64_t lp = (n - 1 + 3) & ~3ull, cp = (n / 2 + 3) & ~3ull;
+    return (2 * lp + 2 * cp) * 4;
+  }
+  return n * 4;  // stwo table pair, or fold twiddles with their sources
+}
+
+uint64_t twiddle_cache_bytes(int device) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  uint64_t b = 0;
+  for (auto& kv : g_cache)
+    if ((int)(kv.first >> 40) == device) b += kv.second->bytes;
+  return b;
 }
 
 int release_twiddles() {

@@ -27,6 +27,7 @@ struct TwiddleSet {
   uint32_t* circle = nullptr;
   uint32_t* icircle = nullptr;
   std::vector<uint32_t> offsets, sizes;  // native per-line-layer (host)
+  uint64_t bytes = 0;                    // device bytes of mem
 };
 
 struct HostCoset {
@@ -43,6 +44,11 @@ int get_twiddles(int kind, uint32_t log_n, const TwiddleSet** out, cudaStream_t 
 // (device, which, log_n).
 int get_fold_twiddles(int which, uint32_t log_n, const uint32_t** out, cudaStream_t st);
 int release_twiddles();
+// Device bytes held by the cached twiddle and fold-twiddle tables of a device.
+uint64_t twiddle_cache_bytes(int device);
+// Bytes get_twiddles(kind, log_n) (kind < 16) or get_fold_twiddles(kind - 16, log_n)
+// would allocate on `device`: 0 when the table is cached.
+uint64_t twiddle_bytes_if_missing(int device, int kind, uint32_t log_n);
 // Frees the cached vanishing-polynomial tables of the Cairo group commit (cairo.cu).
 void release_zh_tables();
 
