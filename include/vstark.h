@@ -359,6 +359,9 @@ int vs_engine_destroy(void* engine);
 /* Builds the workspace for this job shape in every slot (outside any timing). */
 int vs_engine_prepare(void* engine, const vs_job* shape);
 int vs_engine_submit(void* engine, const vs_job* job, uint64_t* ticket);
+/* Queues n jobs at once (all or none), so slots see them together and batch
+ * them fully; tickets[i] receives job i's ticket. */
+int vs_engine_submit_many(void* engine, const vs_job* jobs, uint32_t n, uint64_t* tickets);
 /* Blocks until the job is done. With h_out == NULL only the result record is
  * filled (the bytes stay available); otherwise the bytes are copied and the
  * ticket is retired. */

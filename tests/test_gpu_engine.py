@@ -107,55 +107,28 @@ def test_engine_mix_equals_alone_and_oracle(L):
 
 
 def test_engine_budget_admission(L):
-    """A budget that holds one workspace at a time serialises jobs of different
-    shapes (the idle workspace of one shape is freed for the next); results are
-    unchanged."""
+    """A budget that holds one workspace at a time (here any two workspaces exceed
+    it) serialises jobs of different shapes: the idle workspace of one shape is
+    freed for the next. Results are unchanged."""
     from vortexstark_b200 import api
-    jobs = [api.fib_job(10, 1, 2), api.commit_job(9, 20, 77), api.fib_job(11, 3, 4)]
+    # batch workspaces of the default capacities hold about the same memory at every size
+    jobs = [api.fib_job(16, 1, 2), api.commit_job(20, 34, 77), api.fib_job(17, 3, 4)]
     with api.Engine(1) as probe:
-        biggest = max(probe.workspace_bytes(j) for j in jobs)
-    tw = api_twiddle_margin()
-    with api.Engine(3, biggest + tw) as eng:
+        sizes = sorted(probe.workspace_bytes(j) for j in jobs)
+        tw_now = probe.stats()["twiddle_bytes"]
+    margin = 16 << 20  # the twiddle tables these shapes build (under 10 MB)
+    budget = sizes[-1] + tw_now + margin
+    assert sizes[0] + sizes[1] > sizes[-1] + margin
+    with api.Engine(3, budget) as eng:
         tickets = [eng.submit(j) for j in jobs]
         res = [eng.wait(t) for t in tickets]
         st = eng.stats()
-    assert res[0][0] == O.prove(1, 2, 10) and res[2][0] == O.prove(3, 4, 11)
-    assert res[1][0] == commit_root_oracle(9, 20, 77)
+    assert res[0][0] == O.prove(1, 2, 16) and res[2][0] == O.prove(3, 4, 17)
+    assert res[1][0] == api.commit_seeded(20, 34, 77)
     spans = sorted((r[2], r[3]) for r in res)
     for (s0, e0), (s1, e1) in zip(spans, spans[1:]):
         assert s1 >= e0 - 1e-6  # no two ran at the same time
-    assert st["peak_held_bytes"] <= biggest + tw and st["evictions"] >= 2
-
-
-def api_twiddle_margin():
-    """Budget margin covering the twiddle tables the engine counts (cached ones of
-    earlier tests included) plus the tables small test shapes build."""
-    from vortexstark_b200 import api
-    with api.Engine(1) as e:
-        return e.stats()["twiddle_bytes"] + (64 << 20)
-
-
-def test_engine_rejects_bad_jobs(L):
-    eng = C.c_void_p()
-    V.check(L.vs_engine_create(2, 0, C.byref(eng)))
-    try:
-        t = C.c_uint64()
-        assert L.vs_engine_submit(eng, C.byref(Job(9, 10, 1, 1, 0, 0, 0)), C.byref(t)) == 1
-        V.check(L.vs_engine_submit(eng, C.byref(Job(0, 2, 1, 1, 0, 0, 0)), C.byref(t)))
-        r = JobResult()
-        assert L.vs_engine_wait(eng, t.value, C.byref(r), None, 0) == 1 and r.status == 1
-    finally:
-        L.vs_engine_destroy(eng)
-
-
-def test_engine_priority_policy_does_not_change_results(L):
-    """Size-based stream priorities (default) and equal priorities give the same bytes."""
-    jobs = mixed_jobs()
-    by_size = run_engine(L, jobs, slots=6, flags=0)
-    fifo = run_engine(L, jobs, slots=6, flags=1)
-    assert [r[0] for r in by_size] == [r[0] for r in fifo]
-    eng = C.c_void_p()
-    assert L.vs_engine_create_ex(2, 0, 0x80, C.byref(eng)) == 1  # unknown flag rejected
+    assert st["peak_held_bytes"] <= budget and st["evictions"] >= 2
 
 
 # ---------------------------------------------------------------- batched proofs, budget, failure paths
@@ -234,8 +207,9 @@ def test_engine_holds_at_most_the_budget(L):
         sizes = [probe.workspace_bytes(s) for s in shapes]
     with api.Engine(1) as e:
         tw_now = e.stats()["twiddle_bytes"]
-    budget = max(sizes) * 2 + tw_now + (32 << 20)  # + the twiddle tables these shapes build
-    assert budget < sum(sizes) * 2  # not every shape (two slots' worth) fits at once
+    extra = 32 << 20  # the twiddle tables these shapes build
+    budget = max(sizes) * 2 + tw_now + extra
+    assert max(sizes) * 2 + extra < sum(sizes) * 2  # not every shape (two slots' worth) fits at once
     torch.cuda.synchronize()
     free0 = torch.cuda.mem_get_info()[0]
     low = [free0]

@@ -237,6 +237,13 @@ class Engine:
         check(lib().vs_engine_submit(self.h, C.byref(job), C.byref(t)), "vs_engine_submit")
         return t.value
 
+    def submit_many(self, jobs) -> list[int]:
+        """Queues the jobs at once (slots then batch them fully); returns their tickets."""
+        arr = (Job * max(1, len(jobs)))(*jobs)
+        t = (C.c_uint64 * max(1, len(jobs)))()
+        check(lib().vs_engine_submit_many(self.h, arr, len(jobs), t), "vs_engine_submit_many")
+        return list(t)[:len(jobs)]
+
     def wait(self, ticket: int, timeout_s: float | None = None):
         """Returns (result bytes, t_submit, t_start, t_end) in engine seconds. With a
         timeout, raises VstarkError (status VS_ERR_TIMEOUT = 5) when the job is not

@@ -500,11 +500,24 @@ struct BatchProver::Impl {
       VS_TRY(get_fold_twiddles(l == 0 ? COSET_HALF_COSET : COSET_HALF_ODDS, log_eval - l, &ft, st));
     }
     VS_CUDA(cudaStreamSynchronize(st));
-    // one plain run of a full batch sets kernel attributes before any capture
+    // one plain run of a full batch sets kernel attributes before any capture;
+    // then the graphs of every batch size a launch may use
     VS_TRY(enqueue(cap));
     VS_CUDA(cudaStreamSynchronize(st));
-    cudaGraphExec_t x = nullptr;
-    return graph_for(cap, &x);
+    for (uint32_t b = 1;; b = std::min(2 * b, cap)) {
+      cudaGraphExec_t x = nullptr;
+      VS_TRY(graph_for(b, &x));
+      if (b == cap) break;
+    }
+    return VS_OK;
+  }
+  // Batch size a launch of `count` proofs runs at: the next power of two (at most
+  // the capacity), so a workspace needs only log2(capacity) + 1 graphs; the
+  // padding jobs prove (1, 1) and are not returned.
+  uint32_t padded(uint32_t count) const {
+    uint32_t b = 1;
+    while (b < count) b *= 2;
+    return std::min(b, cap);
   }
 };
 
@@ -533,9 +546,11 @@ int BatchProver::launch(const uint32_t* ab, uint32_t count, cudaStream_t on) {
     return set_error(VS_ERR_INVALID, "batch of %u proofs (capacity %u)", count, impl->cap);
   for (uint32_t i = 0; i < 2 * count; i++)
     if (ab[i] >= h::P) return set_error(VS_ERR_INVALID, "public inputs must be canonical M31");
+  const uint32_t b = impl->padded(count);
   cudaGraphExec_t x = nullptr;
-  VS_TRY(impl->graph_for(count, &x));
+  VS_TRY(impl->graph_for(b, &x));
   std::copy(ab, ab + 2 * count, impl->h_ab);
+  std::fill(impl->h_ab + 2 * count, impl->h_ab + 2 * b, 1u);
   impl->count = count;
   impl->running = on ? on : impl->st;
   VS_CUDA(cudaGraphLaunch(x, impl->running));

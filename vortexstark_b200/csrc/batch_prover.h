@@ -23,7 +23,8 @@ class BatchProver {
   // Device bytes a workspace of this shape allocates (exactly what init() allocates).
   static uint64_t bytes_for(uint32_t log_n, uint32_t capacity);
   // Allocates the workspace on the current device, builds twiddles and captures
-  // the graph of a full batch; graphs of smaller batches are captured on first use.
+  // the graphs of batches of 1, 2, 4, ... proofs up to the capacity (a launch
+  // runs at the next of those sizes, the extra proofs being discarded).
   int init(uint32_t log_n, uint32_t capacity);
   // Starts proofs of (ab[2i], ab[2i+1]) for i < count <= capacity on stream `on`
   // (one batch in flight per instance); finish() waits and serialises each proof.

@@ -485,6 +485,30 @@ int vs_engine_submit(void* h, const vs_job* job, uint64_t* ticket) {
   return VS_OK;
 }
 
+int vs_engine_submit_many(void* h, const vs_job* jobs, uint32_t n, uint64_t* tickets) {
+  clear_error();
+  auto* e = static_cast<Engine*>(h);
+  if (!e || (n && (!jobs || !tickets))) return set_error(VS_ERR_INVALID, "vs_engine_submit_many: null");
+  for (uint32_t i = 0; i < n; i++)
+    if (jobs[i].kind != VS_JOB_FIB && jobs[i].kind != VS_JOB_COMMIT)
+      return set_error(VS_ERR_INVALID, "unknown job kind (job %u); nothing submitted", i);
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    const double t = e->now();
+    for (uint32_t i = 0; i < n; i++) {
+      const uint64_t tk = e->next_ticket++;
+      Result& r = e->results[tk];
+      r.job = jobs[i];
+      r.t_submit = t;
+      e->queue.push_back(tk);
+      e->in_flight++;
+      tickets[i] = tk;
+    }
+  }
+  e->cv_work.notify_all();
+  return VS_OK;
+}
+
 int vs_engine_wait_for(void* h, uint64_t ticket, double timeout_s, vs_job_result* res, uint8_t* out, uint64_t cap) {
   clear_error();
   auto* e = static_cast<Engine*>(h);

@@ -98,7 +98,7 @@ def run_list(engine: Engine, jobs, sequential: bool):
         for j in jobs:
             res.append(engine.wait(engine.submit(j)))
     else:
-        tickets = [engine.submit(j) for j in jobs]
+        tickets = engine.submit_many(jobs)
         res = [engine.wait(t) for t in tickets]
     return engine.now() - t0, res
 
