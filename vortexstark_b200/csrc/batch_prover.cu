@@ -28,6 +28,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "batch_prover.h"
@@ -560,10 +561,19 @@ int BatchProver::launch(const uint32_t* ab, uint32_t count, cudaStream_t on) {
 int BatchProver::finish(std::vector<std::vector<uint8_t>>& out) {
   VS_CUDA(cudaStreamSynchronize(impl->running ? impl->running : impl->st));
   impl->running = nullptr;  // the launch stream may be reused for other work from here on
-  out.resize(impl->count);
-  for (uint32_t j = 0; j < impl->count; j++)
-    impl->lay.serialize(impl->h_arena + (uint64_t)j * impl->lay.words, impl->h_ab[2 * j], impl->h_ab[2 * j + 1],
-                        out[j]);
+  const uint32_t count = impl->count;
+  out.resize(count);
+  auto ser = [&](uint32_t j0, uint32_t step) {
+    for (uint32_t j = j0; j < count; j += step)
+      impl->lay.serialize(impl->h_arena + (uint64_t)j * impl->lay.words, impl->h_ab[2 * j], impl->h_ab[2 * j + 1],
+                          out[j]);
+  };
+  // a batch's proofs are serialised on up to 8 host threads (about 0.1 ms per MB each)
+  const uint32_t nt = std::min<uint32_t>(8, count / 4);
+  std::vector<std::thread> th;
+  for (uint32_t t = 1; t < nt; t++) th.emplace_back(ser, t, nt);
+  ser(0, std::max<uint32_t>(nt, 1));
+  for (auto& x : th) x.join();
   return VS_OK;
 }
 

@@ -248,15 +248,21 @@ void ArenaLayout::plan(uint32_t ln) {
   words = w;
 }
 
-// KRAK v1 from a host copy of the arena (after the stream completed).
-void ArenaLayout::serialize(const uint32_t* A, uint32_t a, uint32_t b, std::vector<uint8_t>& w) const {
-  auto w32 = [&](uint32_t v) { for (int k = 0; k < 4; k++) w.push_back((uint8_t)(v >> (8 * k))); };
-  auto wn = [&](const uint32_t* p, size_t cnt) { for (size_t i = 0; i < cnt; i++) w32(p[i]); };
+// KRAK v1 from a host copy of the arena (after the stream completed). The format
+// is a sequence of little-endian u32 words, so on a little-endian host each field
+// is copied as words: the size is known up front and every region is one memcpy.
+static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "KRAK serialisation copies host words as LE bytes");
+void ArenaLayout::serialize(const uint32_t* A, uint32_t a, uint32_t b, std::vector<uint8_t>& out) const {
+  size_t total = 5 + 16 + 1 + 8 * (size_t)nf + 1 + 32 + 1 + N_QUERIES + 1 + 2 * N_QUERIES + 1 + 2 * N_QUERIES * 4 + 1;
+  for (size_t t = 0; t < depth.size(); t++) total += 2 * N_QUERIES * (1 + (size_t)depth[t] * 8);
+  total += (size_t)nf * (1 + 2 * N_QUERIES * 4);
+  out.resize(total * 4);
+  uint8_t* w = out.data();
+  auto w32 = [&](uint32_t v) { std::memcpy(w, &v, 4); w += 4; };
+  auto wn = [&](const uint32_t* p, size_t cnt) { std::memcpy(w, p, cnt * 4); w += cnt * 4; };
   auto wpaths = [&](size_t off, uint32_t d, uint32_t s) {
     for (uint32_t qi = 0; qi < N_QUERIES; qi++) { w32(d); wn(A + off + ((size_t)(s * N_QUERIES + qi) * d) * 8, (size_t)d * 8); }
   };
-  w.clear();
-  w.reserve(words * 4 + 4096);
   w32(0x4B52414Bu); w32(1); w32(log_n); w32(a); w32(b);
   wn(A + roots, 16);
   w32(nf);

