@@ -534,6 +534,29 @@ def mix_parity(jobs, results):
     return "digest-match"
 
 
+def profile_batch(log_n: int) -> None:
+    """One batch of 64 Fibonacci proofs on one slot (batch limit 64) inside a profiler
+    range, after preparing the workspace and one warm batch; checks the first proof
+    against the plain path."""
+    import torch
+
+    from vortexstark_b200 import api
+    from vortexstark_b200 import workloads as W
+    jobs = W.plain_jobs(64, log_n)
+    with api.Engine(1, size_priority=False) as eng:
+        eng.set_batch_limit(64)
+        eng.prepare(jobs[0])
+        W.run_list(eng, jobs, sequential=False)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        t, r = W.run_list(eng, jobs, sequential=False)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+    if r[0][0] != api.prove_fib(jobs[0].a, jobs[0].b, log_n):
+        raise SystemExit("profile batch: proof differs from the plain path")
+    print(json.dumps({"profile_batch": {"log_n": log_n, "proofs": len(jobs), "ms": t * 1e3}}))
+
+
 # ---------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -561,7 +584,12 @@ def main():
                     help="trace sizes (log) the NTT autotuner tunes before the timed runs")
     ap.add_argument("--prove-sizes", type=int, nargs="*", default=[20, 24, 28],
                     help="log_n of the single-proof latency runs")
+    ap.add_argument("--profile-batch", type=int, default=None, metavar="LOG_N",
+                    help="profiler run only: one warm batch of 64 Fibonacci proofs of 2^LOG_N rows, then one batch "
+                         "inside cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
+    if args.profile_batch is not None:
+        return profile_batch(args.profile_batch)
     args.warmup = max(args.warmup, 3)
     if args.cpu_log_n is None:
         args.cpu_log_n = 20 if args.impl == "reference" else 22
@@ -682,6 +710,33 @@ def main():
     three = {"groups": "/".join(str(b - a) for a, b in groups), "ms": m0.elapsed_time(m1) / args.steps,
              "row_packed_root_ms": phase["merkle"]}
 
+    # Does the row-packed root pay for reading the LDE back from HBM? The same
+    # launch (34 columns x 2^19 rows, 71 MB) hashed back to back from one buffer,
+    # which stays in the 126 MB L2, against rotating over four such buffers (285 MB,
+    # so each launch reads its columns from HBM). Equal times mean the re-read is
+    # hidden behind the hashing, so fusing the LDE with the leaf hash could not
+    # shorten the step.
+    rows = 1 << 19
+    bufs = [lde[:, k * rows:(k + 1) * rows].contiguous() for k in range(4)]
+    root_p = torch.zeros(8, dtype=torch.int32, device="cuda")
+
+    def timed(pick, reps=40):
+        for k in range(4):
+            api.merkle_root_rowpacked(bufs[pick(k)], root_p)
+        torch.cuda.synchronize()
+        m0.record(st)
+        for k in range(reps):
+            api.merkle_root_rowpacked(bufs[pick(k)], root_p)
+        m1.record(st)
+        torch.cuda.synchronize()
+        return m0.elapsed_time(m1) / reps
+
+    warm_ms, cold_ms = timed(lambda k: 0), timed(lambda k: k % 4)
+    fusion = {"workload": f"row-packed root of {n_cols} columns x 2^19 rows: one L2-resident buffer vs four "
+                          "buffers in rotation (read from HBM)",
+              "l2_resident_ms": warm_ms, "hbm_ms": cold_ms, "hbm_over_l2": cold_ms / warm_ms}
+    del bufs
+
     oods = oods_quotients(args, V, torch, lde, N, st, ev) if rank == 0 and not args.no_oods else None
     folds = fold_dropins(args, V, torch, fri_src, ev) if rank == 0 and not args.no_oods else None
 
@@ -782,7 +837,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic (seeded SplitMix64 uniform M31)",
                 "config": config_json(args), "parity": parity, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": clk.summary(), "three_tree_commit": three, "oods": oods, "fri_fold_dropins": folds, "ntt_autotune": tuning,
+                "gpu_launches": launches, "clocks": clk.summary(), "three_tree_commit": three, "lde_leaf_fusion_probe": fusion, "oods": oods, "fri_fold_dropins": folds, "ntt_autotune": tuning,
                 "cairo": cairo, "proofs": proofs}
         print(json.dumps(line), flush=True)
     replicas.finalize()
