@@ -197,6 +197,20 @@ void cuda_accumulate_lift(uint32_t* col, const uint32_t* curr, uint32_t col_n, u
  * device arrays of device pointers (4 and 64 of them) (src/cuda/ffi.rs:960-964;
  * cuda/pack_leaves.cu:44-52; caller merkle_ops.rs:193). */
 void cuda_pack_leaves(const uint32_t* const* input_col_ptrs, uint32_t* const* output_col_ptrs, uint32_t n);
+/* FRI fold twiddles of a stwo domain, built on the device (the adapter builds them
+ * on the host for every fold: crates/cuda-backend/src/fri_ops.rs:50-56 for the
+ * circle fold, :100-106 for line folds). With is_line = 0 the domain is the source
+ * evaluation's CircleDomain of 2^log_size points, given by its half coset (initial
+ * point, step): d_out[i] = 1 / y(half_coset.at(bit_reverse_index(2i, log_size))).
+ * With is_line = 1 it is a LineDomain of 2^log_size points given by its coset:
+ * d_out[i] = 1 / x(coset.at(bit_reverse_index(2i, log_size))). i < 2^(log_size-1);
+ * a zero coordinate maps to 0 (chunked batch inverse). Stream-ordered. */
+int vs_fold_twiddles_stwo(uint32_t is_line, uint32_t init_x, uint32_t init_y, uint32_t step_x, uint32_t step_y,
+                          uint32_t log_size, uint32_t* d_out, vs_stream_t stream);
+/* Domain points of CanonicCoset(log_size)'s circle domain in bit-reversed row
+ * order, d_xs[r], d_ys[r] = domain.at(bit_reverse_index(r, log_size)), built on the
+ * device (the adapter builds them on the host per call: quotient_ops.rs:135-140). */
+int vs_canonic_domain_points(uint32_t log_size, uint32_t* d_xs, uint32_t* d_ys, vs_stream_t stream);
 
 /* ===================================================================== */
 /* 2. vs_* entry points (no reference counterpart)                        */

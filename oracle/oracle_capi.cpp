@@ -220,6 +220,17 @@ void oracle_fold_twiddles(uint32_t kind, uint32_t log_n, int extract_y, uint32_t
   auto t = fold_twiddles(make_coset(kind, log_n), extract_y != 0);
   std::memcpy(out, t.data(), t.size() * 4);
 }
+// Row r of CanonicCoset(log_size)'s circle domain at bit_reverse_index(r): the
+// domain points the stwo adapter builds per call (crates/cuda-backend/src/
+// quotient_ops.rs:135-140; CircleDomain::at over half_odds(log_size - 1)).
+void oracle_canonic_domain_points(uint32_t log_size, uint32_t* xs, uint32_t* ys) {
+  const uint64_t n = 1ull << log_size;
+  for (uint64_t r = 0; r < n; r++) {
+    const CPoint p = canonic_domain_point(bit_reverse(r, log_size), log_size);
+    xs[r] = p.x;
+    ys[r] = p.y;
+  }
+}
 // Generic coset (matches cuda_compute_fold_twiddle_sources + cuda_batch_inverse_m31).
 void oracle_fold_twiddles_generic(uint32_t ix, uint32_t iy, uint32_t sx, uint32_t sy, uint32_t log_n, int extract_y,
                                   uint32_t* out) {

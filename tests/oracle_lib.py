@@ -372,6 +372,13 @@ def fold_twiddles(kind: int, log_n: int, extract_y: bool) -> np.ndarray:
     return o
 
 
+def canonic_domain_points(log_size: int):
+    xs = np.empty(1 << log_size, np.uint32)
+    ys = np.empty(1 << log_size, np.uint32)
+    lib().oracle_canonic_domain_points(log_size, ptr(xs), ptr(ys))
+    return xs, ys
+
+
 def fold_twiddles_generic(ix, iy, sx, sy, log_n, extract_y) -> np.ndarray:
     o = np.empty(1 << (log_n - 1), np.uint32)
     lib().oracle_fold_twiddles_generic(ix, iy, sx, sy, log_n, int(extract_y), ptr(o))

@@ -109,3 +109,43 @@ def test_pack_leaves(L, n, off):
     L.cuda_pack_leaves(ptr(ptr_array(ins)), ptr(ptr_array(outs)), n)
     got = np.stack([host(o) for o in outs])
     assert np.array_equal(got, O.pack_leaves(cols))
+
+
+# ---- domain helpers behind the adapter (fri_ops.rs:50-56,100-106; quotient_ops.rs:135-140)
+@pytest.mark.parametrize("log_size", [1, 2, 4, 9, 13, 16, 20])
+def test_canonic_domain_points(L, log_size):
+    n = 1 << log_size
+    xs, ys = zeros(n), zeros(n)
+    V.check(L.vs_canonic_domain_points(log_size, ptr(xs), ptr(ys), None), "vs_canonic_domain_points")
+    ex, ey = O.canonic_domain_points(log_size)
+    assert np.array_equal(host(xs), ex) and np.array_equal(host(ys), ey)
+
+
+def _coset(kind, log_size):
+    c = O.coset(kind, log_size)
+    return c[0], c[1], c[2], c[3]
+
+
+@pytest.mark.parametrize("log_size", [1, 4, 7, 12, 16, 20])
+@pytest.mark.parametrize("is_line", [0, 1])
+def test_fold_twiddles_stwo(L, log_size, is_line):
+    """Circle: the half coset of CanonicCoset(log_size)'s domain (half_odds(log_size-1));
+    line: the coset half_odds(log_size) of a 2^log_size-point line domain; and, for
+    both, the coset half_coset(log_size) (whose small sizes hold points with a zero
+    coordinate, which map to 0 on both sides)."""
+    half = 1 << (log_size - 1)
+    cosets = [_coset(O.HALF_ODDS, log_size - 1) if not is_line else _coset(O.HALF_ODDS, log_size)]
+    hc = _coset(O.HALF_COSET, log_size)
+    cosets.append((hc[0], hc[1], hc[2], hc[3]))
+    for ix, iy, sx, sy in cosets:
+        out = zeros(half)
+        V.check(L.vs_fold_twiddles_stwo(is_line, ix, iy, sx, sy, log_size, ptr(out), None), "vs_fold_twiddles_stwo")
+        exp = O.fold_twiddles_generic(ix, iy, sx, sy, log_size, not is_line)
+        assert np.array_equal(host(out), exp)
+
+
+def test_domain_helpers_reject_bad_arguments(L):
+    out = zeros(8)
+    assert L.vs_fold_twiddles_stwo(0, P, 0, 1, 0, 4, ptr(out), None) == 1
+    assert L.vs_fold_twiddles_stwo(0, 1, 0, 1, 0, 0, ptr(out), None) == 1
+    assert L.vs_canonic_domain_points(31, ptr(out), ptr(out), None) == 1

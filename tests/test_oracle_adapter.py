@@ -63,3 +63,70 @@ def test_pack_leaves(n):
     if n % 16 == 0:
         # the stwo PackLeaves layout: output column 16c + p holds input c's words p, p+16, ...
         assert np.array_equal(got.reshape(4, 16, n // 16), cols.reshape(4, n // 16, 16).transpose(0, 2, 1))
+
+
+# ---- domain helpers behind the adapter (fri_ops.rs:50-56,100-106; quotient_ops.rs:135-140)
+G = (2, 1268011823)
+
+
+def _pmul(a, b):
+    return ((a[0] * b[0] - a[1] * b[1]) % P, (a[0] * b[1] + a[1] * b[0]) % P)
+
+
+def _dbl(p, k):
+    for _ in range(k):
+        p = _pmul(p, p)
+    return p
+
+
+def _ppow(p, e):
+    r = (1, 0)
+    while e:
+        if e & 1:
+            r = _pmul(r, p)
+        p = _pmul(p, p)
+        e >>= 1
+    return r
+
+
+def _brev(i, bits):
+    return int(format(i, f"0{bits}b")[::-1], 2) if bits else 0
+
+
+def _half_odds(l):
+    return _dbl(G, 29 - l if l < 29 else 0), _dbl(G, 31 - l)
+
+
+def _circle_domain_at(half, i, log_size):
+    """stwo CircleDomain::at: half_coset.at(i) for i < 2^(log_size-1), else its conjugate."""
+    init, step = half
+    h = 1 << (log_size - 1)
+    p = _pmul(init, _ppow(step, i % h))
+    return p if i < h else (p[0], (-p[1]) % P)
+
+
+@pytest.mark.parametrize("log_size", [1, 2, 3, 5, 8])
+def test_canonic_domain_points_restatement(log_size):
+    xs, ys = O.canonic_domain_points(log_size)
+    half = _half_odds(log_size - 1)
+    for r in range(1 << log_size):
+        assert (int(xs[r]), int(ys[r])) == _circle_domain_at(half, _brev(r, log_size), log_size)
+        assert (int(xs[r]) ** 2 + int(ys[r]) ** 2) % P == 1
+    assert len(set(zip(xs.tolist(), ys.tolist()))) == 1 << log_size
+
+
+@pytest.mark.parametrize("log_size", [2, 4, 7])
+def test_fold_twiddles_of_stwo_domains(log_size):
+    """1/y of CircleDomain.at(brev(2i)) and 1/x of LineDomain.at(brev(2i)): the
+    generic coset formula (initial * step^brev(2i)) covers both, because every
+    bit-reversed even index lies in the domain's first half."""
+    half = _half_odds(log_size - 1)  # CanonicCoset(log_size).circle_domain()
+    got = O.fold_twiddles_generic(*half[0], *half[1], log_size, True)
+    for i in range(1 << (log_size - 1)):
+        y = _circle_domain_at(half, _brev(2 * i, log_size), log_size)[1]
+        assert int(got[i]) == pow(y, P - 2, P)
+    line = _half_odds(log_size)  # a line domain of 2^log_size points
+    got = O.fold_twiddles_generic(*line[0], *line[1], log_size, False)
+    for i in range(1 << (log_size - 1)):
+        x = _pmul(line[0], _ppow(line[1], _brev(2 * i, log_size)))[0]
+        assert int(got[i]) == pow(x, P - 2, P)

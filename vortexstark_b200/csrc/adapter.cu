@@ -7,6 +7,8 @@
 // Indexing is 64-bit throughout; the reference computes some element offsets in
 // 32 bits (gather.cu:32, barycentric_eval.cu:43, accumulate_lift.cu:29), so the
 // two agree on every size where those offsets fit in 32 bits.
+#include "host_math.h"
+#include "twiddles.h"
 #include "vs_common.cuh"
 #include "vs_field.cuh"
 #include "vs_mem.cuh"
@@ -171,6 +173,52 @@ __global__ void pack_leaves_kernel(const uint32_t* const* __restrict__ in_ptrs, 
   }
 }
 
+// ---- domain helpers the adapter computes on the host per call (fri_ops.rs:50-56,
+// 100-106; quotient_ops.rs:135-140), built on the device instead.
+// step^(2^b) for b < 31, so step^e costs popcount(e) circle multiplications.
+struct PowTable {
+  cpt p[31];
+};
+PowTable pow_table(h::Pt step) {
+  PowTable t;
+  for (int b = 0; b < 31; b++) {
+    t.p[b] = cpt{step.x, step.y};
+    step = h::pmul(step, step);
+  }
+  return t;
+}
+__device__ __forceinline__ cpt pow_bits(const PowTable& t, uint32_t e) {
+  cpt r{1, 0};
+  for (int b = 0; e; b++, e >>= 1)
+    if (e & 1) r = cpmul(r, t.p[b]);
+  return r;
+}
+
+// out[i] = coord(initial * step^brev_L(2i)), i < 2^(L-1): x for line domains, y for
+// the half coset of a circle domain (the domains' own at(), stwo CircleDomain::at
+// and LineDomain::at, whose bit-reversed even indices all lie in the first half).
+__global__ void fold_points_kernel(cpt initial, PowTable t, uint32_t L, int extract_y, uint32_t* __restrict__ out) {
+  const uint32_t half = 1u << (L - 1);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < half; i += gridDim.x * blockDim.x) {
+    const cpt p = cpmul(initial, pow_bits(t, brev(i << 1, L)));
+    out[i] = extract_y ? p.y : p.x;
+  }
+}
+
+// Row r of CanonicCoset(L)'s circle domain in bit-reversed order: j = brev_L(r);
+// half_odds(L-1).at(j) for j < 2^(L-1), its conjugate at j - 2^(L-1) otherwise
+// (stwo CircleDomain::at over the canonic half coset).
+__global__ void canonic_domain_points_kernel(cpt initial, PowTable t, uint32_t L, uint32_t* __restrict__ xs,
+                                             uint32_t* __restrict__ ys) {
+  const uint32_t n = 1u << L, half = n >> 1;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const uint32_t j = brev(r, L);
+    const cpt p = cpmul(initial, pow_bits(t, j & (half - 1)));
+    xs[r] = p.x;
+    ys[r] = j >= half ? neg(p.y) : p.y;
+  }
+}
+
 }  // namespace
 }  // namespace vs
 
@@ -223,6 +271,37 @@ void cuda_pack_leaves(const uint32_t* const* input_col_ptrs, uint32_t* const* ou
   if (gx > cap) gx = cap;
   pack_leaves_kernel<<<dim3(gx, 4), kThreads>>>(input_col_ptrs, output_col_ptrs, n);
   check_cuda(cudaGetLastError(), "cuda_pack_leaves");
+}
+
+
+// FRI fold twiddles of a stwo domain (fri_ops.rs:50-56 circle, :100-106 line),
+// one launch plus the chunked batch inverse, stream-ordered.
+int vs_fold_twiddles_stwo(uint32_t is_line, uint32_t init_x, uint32_t init_y, uint32_t step_x, uint32_t step_y,
+                          uint32_t log_size, uint32_t* d_out, vs_stream_t stream) {
+  clear_error();
+  if (!d_out) return set_error(VS_ERR_INVALID, "vs_fold_twiddles_stwo: null output");
+  if (log_size < 1 || log_size > 31) return set_error(VS_ERR_INVALID, "vs_fold_twiddles_stwo: log_size %u", log_size);
+  if (init_x >= VS_P || init_y >= VS_P || step_x >= VS_P || step_y >= VS_P)
+    return set_error(VS_ERR_INVALID, "vs_fold_twiddles_stwo: coordinates must be canonical M31");
+  cudaStream_t st = (cudaStream_t)stream;
+  const uint32_t half = 1u << (log_size - 1);
+  fold_points_kernel<<<stride_grid(half, kThreads), kThreads, 0, st>>>(cpt{init_x, init_y},
+                                                                      pow_table(h::Pt{step_x, step_y}), log_size,
+                                                                      is_line ? 0 : 1, d_out);
+  VS_LAUNCHED("fold_points_kernel");
+  return launch_batch_inverse(d_out, d_out, half, st);
+}
+
+// BRT-canonic domain points of CanonicCoset(log_size) (quotient_ops.rs:135-140).
+int vs_canonic_domain_points(uint32_t log_size, uint32_t* d_xs, uint32_t* d_ys, vs_stream_t stream) {
+  clear_error();
+  if (!d_xs || !d_ys) return set_error(VS_ERR_INVALID, "vs_canonic_domain_points: null output");
+  if (log_size < 1 || log_size > 30) return set_error(VS_ERR_INVALID, "vs_canonic_domain_points: log_size %u", log_size);
+  const h::Coset ho = h::half_odds(log_size - 1);
+  canonic_domain_points_kernel<<<stride_grid(1ull << log_size, kThreads), kThreads, 0, (cudaStream_t)stream>>>(
+      cpt{ho.initial.x, ho.initial.y}, pow_table(ho.step), log_size, d_xs, d_ys);
+  VS_LAUNCHED("canonic_domain_points_kernel");
+  return VS_OK;
 }
 
 }  // extern "C"

@@ -199,7 +199,15 @@ struct Engine {
     p.key = key_of(j);
     p.picks.push_back(head);
     if (batched(j)) {
-      const uint32_t cap = batch_capacity(j.log_n);
+      // queued jobs of this size are shared among the slots that are free now
+      // (concurrent batches keep the GPU busier than one large batch and a wait)
+      uint32_t same = 0;
+      for (auto it = head; it != queue.end(); ++it) {
+        const vs_job& o = results[*it].job;
+        same += o.kind == j.kind && o.log_n == j.log_n;
+      }
+      const uint32_t free_slots = std::max<uint32_t>(1, (uint32_t)slots.size() - busy);
+      const uint32_t cap = std::min(batch_capacity(j.log_n), (same + free_slots - 1) / free_slots);
       for (auto it = std::next(head); it != queue.end() && p.picks.size() < cap; ++it) {
         const vs_job& o = results[*it].job;
         if (o.kind == j.kind && o.log_n == j.log_n &&
