@@ -464,6 +464,47 @@ int vs_stwo_fri_witness(const uint64_t* h_positions, uint32_t n, const uint32_t*
 int vs_stwo_root_from_witness(uint32_t log_height, const uint64_t* h_positions, uint32_t n, const uint32_t* h_rows,
                               uint32_t n_cols, const uint32_t* h_witness, uint32_t n_witness, uint32_t* h_root);
 
+/* The stwo wire-format proof (src/stwo_export.rs:415-660 cairo_proof_to_stwo and
+ * :687-690 cairo_proof_to_json): the seven commitment trees in channel order
+ * (trace columns 0-15, 16-30 and 31-33, the LogUp, RC and S_dict interaction trees,
+ * the composition quotient), their OODS samples, column-major queried values and
+ * deduplicated hash witnesses (the trace trees over the query rows and, when next-row
+ * paths are given, the next rows), and the FRI proof (the OODS quotient as first
+ * layer with its fold-pair witness, then each line-fold layer). All arrays are host
+ * memory; auth paths are [query][level][8 words], leaf level first, with
+ * height = log_trace_size + 2 (FRI layer i: height - i - 1). */
+typedef struct {
+  uint32_t log_trace_size;
+  uint32_t n_queries;
+  const uint64_t* query_indices;            /* n_queries positions in the evaluation domain */
+  uint64_t pow_nonce;
+  uint32_t commitments[7][8];
+  uint32_t n_trace_cols;                    /* >= 16; columns past 34 are not exported */
+  const uint32_t* trace_values_at_queries;  /* [n_queries][n_trace_cols] */
+  uint32_t n_oods, n_oods_next;             /* trace columns sampled at z and at z_next */
+  const uint32_t* oods_trace_at_z;          /* [n_oods][4] */
+  const uint32_t* oods_trace_at_z_next;     /* [n_oods_next][4] */
+  uint32_t oods_interaction_at_z[3][4][4];  /* all zero: not sampled */
+  uint32_t oods_interaction_at_z_next[3][4][4];
+  uint32_t oods_quotient_at_z[4][4];        /* all zero: not sampled */
+  const uint32_t* trace_auth_paths[3];      /* trees 0-2 at the query rows */
+  const uint32_t* trace_auth_paths_next[3]; /* at the next rows, or NULL */
+  const uint32_t* decom_values[4];          /* trees 3-6: [n_queries][4] */
+  const uint32_t* decom_auth_paths[4];
+  uint32_t oods_quotient_commitment[8];
+  const uint32_t* oods_quotient_sibling_values;  /* [n_queries][4] at position ^ 1 */
+  const uint32_t* oods_quotient_auth_paths;
+  uint32_t n_fri;
+  const uint32_t* fri_commitments;          /* [n_fri][8] */
+  const uint32_t* const* fri_sibling_values; /* n_fri host arrays [n_queries][4] */
+  const uint32_t* const* fri_auth_paths;    /* n_fri host arrays [n_queries][height - i - 1][8] */
+  uint32_t n_last;
+  const uint32_t* last_layer_poly;          /* [n_last][4] */
+} vs_stwo_proof_parts;
+/* Writes the proof as serde_json's pretty JSON into h_out (when cap suffices);
+ * *out_len receives its length (h_out NULL: length query). */
+int vs_stwo_proof_json(const vs_stwo_proof_parts* parts, char* h_out, uint64_t cap, uint64_t* out_len);
+
 /* Circle polynomials in the stwo coefficient basis evaluated at QM31 points
  * (oods.rs:133-161, eval_at_oods_from_coeffs, which the reference runs on the
  * host per column). h_cols: host array of n_cols device pointers, 2^log_len

@@ -428,3 +428,83 @@ def cairo_oods_fri(channel: Channel, log_n: int, trace_coeffs, trace_evals, inte
         "fri_alphas": q(io.fri_alphas, log_n - 1), "last_layer": q(io.last_layer, 8),
         "last_layer_coeffs": q(io.last_layer_coeffs, 8),
     }
+
+
+# ------------------------------------------------------------------ stwo wire-format export (src/stwo_export.rs)
+class StwoProofParts(C.Structure):
+    """Mirror of vs_stwo_proof_parts (include/vstark.h)."""
+    _fields_ = [
+        ("log_trace_size", C.c_uint32), ("n_queries", C.c_uint32), ("query_indices", C.c_void_p),
+        ("pow_nonce", C.c_uint64), ("commitments", (C.c_uint32 * 8) * 7), ("n_trace_cols", C.c_uint32),
+        ("trace_values_at_queries", C.c_void_p), ("n_oods", C.c_uint32), ("n_oods_next", C.c_uint32),
+        ("oods_trace_at_z", C.c_void_p), ("oods_trace_at_z_next", C.c_void_p),
+        ("oods_interaction_at_z", ((C.c_uint32 * 4) * 4) * 3),
+        ("oods_interaction_at_z_next", ((C.c_uint32 * 4) * 4) * 3),
+        ("oods_quotient_at_z", (C.c_uint32 * 4) * 4), ("trace_auth_paths", C.c_void_p * 3),
+        ("trace_auth_paths_next", C.c_void_p * 3), ("decom_values", C.c_void_p * 4),
+        ("decom_auth_paths", C.c_void_p * 4), ("oods_quotient_commitment", C.c_uint32 * 8),
+        ("oods_quotient_sibling_values", C.c_void_p), ("oods_quotient_auth_paths", C.c_void_p),
+        ("n_fri", C.c_uint32), ("fri_commitments", C.c_void_p), ("fri_sibling_values", C.c_void_p),
+        ("fri_auth_paths", C.c_void_p), ("n_last", C.c_uint32), ("last_layer_poly", C.c_void_p),
+    ]
+
+
+def stwo_proof_json(parts: dict) -> str:
+    """The stwo-compatible JSON proof (cairo_proof_to_json) from proof parts given as
+    numpy uint32 arrays (query_indices uint64): keys as in vs_stwo_proof_parts;
+    trace_auth_paths / trace_auth_paths_next / decom_values / decom_auth_paths are
+    lists (None entries allowed for the next-row paths); fri_sibling_values and
+    fri_auth_paths are lists of per-layer arrays."""
+    import numpy as np
+    keep = []
+
+    def arr(a, dtype=np.uint32):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype)
+        keep.append(a)
+        return a.ctypes.data
+
+    p = StwoProofParts()
+    q = np.ascontiguousarray(parts["query_indices"], np.uint64)
+    p.log_trace_size, p.n_queries, p.query_indices = parts["log_trace_size"], len(q), arr(q, np.uint64)
+    p.pow_nonce = int(parts.get("pow_nonce", 0))
+    for t, h in enumerate(parts["commitments"]):
+        p.commitments[t][:] = [int(x) for x in h]
+    tv = np.ascontiguousarray(parts["trace_values_at_queries"], np.uint32)
+    p.n_trace_cols, p.trace_values_at_queries = (tv.shape[1] if tv.ndim == 2 else 0), arr(tv)
+    z, zn = parts.get("oods_trace_at_z"), parts.get("oods_trace_at_z_next")
+    p.n_oods = 0 if z is None else len(z)
+    p.n_oods_next = 0 if zn is None else len(zn)
+    p.oods_trace_at_z, p.oods_trace_at_z_next = arr(z), arr(zn)
+    for name in ("oods_interaction_at_z", "oods_interaction_at_z_next"):
+        v = np.zeros((3, 4, 4), np.uint32) if parts.get(name) is None else np.asarray(parts[name], np.uint32)
+        for a in range(3):
+            for b in range(4):
+                getattr(p, name)[a][b][:] = [int(x) for x in v[a, b]]
+    qz = np.zeros((4, 4), np.uint32) if parts.get("oods_quotient_at_z") is None else np.asarray(parts["oods_quotient_at_z"])
+    for a in range(4):
+        p.oods_quotient_at_z[a][:] = [int(x) for x in qz[a]]
+    for t in range(3):
+        p.trace_auth_paths[t] = arr(parts["trace_auth_paths"][t])
+        nxt = parts.get("trace_auth_paths_next")
+        p.trace_auth_paths_next[t] = arr(nxt[t]) if nxt is not None else None
+    for t in range(4):
+        p.decom_values[t] = arr(parts["decom_values"][t])
+        p.decom_auth_paths[t] = arr(parts["decom_auth_paths"][t])
+    p.oods_quotient_commitment[:] = [int(x) for x in parts["oods_quotient_commitment"]]
+    p.oods_quotient_sibling_values = arr(parts["oods_quotient_sibling_values"])
+    p.oods_quotient_auth_paths = arr(parts["oods_quotient_auth_paths"])
+    fc = parts.get("fri_commitments", [])
+    p.n_fri, p.fri_commitments = len(fc), arr(np.asarray(fc, np.uint32).reshape(-1, 8) if len(fc) else None)
+    sv = [arr(x) for x in parts.get("fri_sibling_values", [])]
+    ap = [arr(x) for x in parts.get("fri_auth_paths", [])]
+    sva, apa = (C.c_void_p * max(1, len(sv)))(*sv), (C.c_void_p * max(1, len(ap)))(*ap)
+    p.fri_sibling_values, p.fri_auth_paths = C.cast(sva, C.c_void_p), C.cast(apa, C.c_void_p)
+    last = parts.get("last_layer_poly")
+    p.n_last, p.last_layer_poly = (0 if last is None else len(last)), arr(last)
+    n = C.c_uint64()
+    check(lib().vs_stwo_proof_json(C.byref(p), None, 0, C.byref(n)), "vs_stwo_proof_json")
+    buf = C.create_string_buffer(n.value + 1)
+    check(lib().vs_stwo_proof_json(C.byref(p), buf, n.value + 1, C.byref(n)), "vs_stwo_proof_json")
+    return buf.raw[: n.value].decode()
