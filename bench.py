@@ -817,6 +817,8 @@ def main():
             # schedulers x 32 lanes x the sampled SM clock.
             "int_issue_frac": (-(-n_cols * 4 // 64) + 1) * 1179 * N / (phase["merkle"] / 1e3)
                               / (148 * 4 * 32 * clk_hz),
+            "int_issue_basis": "derived: 1179 instructions per compression from one ncu count "
+                               "(profiles/merkle_rowpacked_fold_log22.md), not measured in this run",
             "launch_ms": phase["merkle"], "phase_ms": phase,
             "phase_hbm_frac": {k: alg[k] / (phase[k] / 1e3) / 1e9 / hbm for k in phase}}
 
