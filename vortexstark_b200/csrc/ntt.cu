@@ -529,13 +529,17 @@ __device__ __forceinline__ void rbfly4_t(uint4 (&v)[8], const uint32_t (&t)[8]) 
 // top pass; the working tile itself in a pass kernel).
 template <int M, int C, int r, int S0 = C>
 __device__ __forceinline__ void inv_rounds4(uint32_t* sm, uint32_t* cf, const TileGeo& g, const NttTw& tw,
-                                            uint32_t scale, uint32_t (&t)[8]) {
+                                            uint32_t scale, uint32_t (&t)[8], const TileGeo& gn,
+                                            const NttTw& twn) {
   constexpr int TOP = Tile4<M, C, S0>::NR - 1;
   uint32_t tn[8];
   if constexpr (r < TOP) tw4_fetch<M, C, r + 1, S0>(tn, g, tw);
   uint4 v[8];
   rload4<M, C, r, S0>(v, sm);
   rbfly4_t<false, M, C, r, S0>(v, t);
+  // t is free once the last round's butterflies are done: fetch the forward
+  // pass's first-round twiddles into it, ahead of the scale, stores and barrier
+  if constexpr (r == TOP) tw4_fetch<M, C, TOP, S0>(t, gn, twn);
   if constexpr (r == TOP) {
     if (scale) {
 #pragma unroll
@@ -554,7 +558,7 @@ __device__ __forceinline__ void inv_rounds4(uint32_t* sm, uint32_t* cf, const Ti
   if constexpr (r < TOP) {
 #pragma unroll
     for (int k = 0; k < 8; k++) t[k] = tn[k];
-    inv_rounds4<M, C, r + 1, S0>(sm, cf, g, tw, scale, t);
+    inv_rounds4<M, C, r + 1, S0>(sm, cf, g, tw, scale, t, gn, twn);
   }
 }
 // Forward chunk rounds r..0 (round TOP reads from cf: the parked coefficients of
@@ -562,19 +566,24 @@ __device__ __forceinline__ void inv_rounds4(uint32_t* sm, uint32_t* cf, const Ti
 // ahead as above.
 template <int M, int C, int r, int S0 = C>
 __device__ __forceinline__ void fwd_rounds4(uint32_t* sm, const uint32_t* cf, const TileGeo& g, const NttTw& tw,
-                                            uint32_t (&t)[8]) {
+                                            uint32_t (&t)[8], const TileGeo& gn, bool next) {
   constexpr int TOP = Tile4<M, C, S0>::NR - 1;
   uint32_t tn[8];
   if constexpr (r > 0) tw4_fetch<M, C, (r > 0 ? r - 1 : 0), S0>(tn, g, tw);
   uint4 v[8];
   rload4<M, C, r, S0>(v, r == TOP ? cf : sm);
   rbfly4_t<true, M, C, r, S0>(v, t);
+  // after the block's last butterflies t is free: fetch the next block's
+  // first-round twiddles into it, ahead of the stores, barrier and tile store
+  if constexpr (r == 0) {
+    if (next) tw4_fetch<M, C, TOP, S0>(t, gn, tw);
+  }
   rstore4<M, C, r, S0>(v, sm);  // the previous block's tile_store finished before the block-end barrier
   __syncthreads();
   if constexpr (r > 0) {
 #pragma unroll
     for (int k = 0; k < 8; k++) t[k] = tn[k];
-    fwd_rounds4<M, C, (r > 0 ? r - 1 : 0), S0>(sm, cf, g, tw, t);
+    fwd_rounds4<M, C, (r > 0 ? r - 1 : 0), S0>(sm, cf, g, tw, t, gn, next);
   }
 }
 
@@ -597,20 +606,21 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPa
   tw4_fetch<M, C, 0>(t, gi, inv.tw);
   tile_load4<M, C>(sm, col_src(inv, blockIdx.y), gi, inv.src_mask);
   __syncthreads();
-  inv_rounds4<M, C, 0>(sm, cf, gi, inv.tw, inv.scale, t);
   uint32_t* dst = col_dst(fwd, blockIdx.y);
   TileGeo gf = gi;
   gf.hi = 0;
   gf.gbase = gi.gbase;
-  tw4_fetch<M, C, TOP>(t, gf, fwd.tw);
+  // each block's first-round twiddles are fetched right after the butterflies of
+  // the round before it (the last inverse round, then each block's round 0)
+  inv_rounds4<M, C, 0>(sm, cf, gi, inv.tw, inv.scale, t, gf, fwd.tw);
   for (uint32_t q = 0; q < (1u << B); q++) {
-    fwd_rounds4<M, C, TOP>(sm, cf, gf, fwd.tw, t);
     const TileGeo gq = gf;
-    if (q + 1 < (1u << B)) {
+    const bool more = q + 1 < (1u << B);
+    if (more) {
       gf.hi = q + 1;
       gf.gbase = ((q + 1) << (gi.a + M)) | gi.gbase;
-      tw4_fetch<M, C, TOP>(t, gf, fwd.tw);
     }
+    fwd_rounds4<M, C, TOP>(sm, cf, gq, fwd.tw, t, gf, more);
     tile_store4<M, C>(sm, dst, gq);
     __syncthreads();
   }
