@@ -578,7 +578,11 @@ __device__ __forceinline__ void fwd_rounds4(uint32_t* sm, const uint32_t* cf, co
   if constexpr (r == 0) {
     if (next) tw4_fetch<M, C, TOP, S0>(t, gn, tw);
   }
-  rstore4<M, C, r, S0>(v, sm);  // the previous block's tile_store finished before the block-end barrier
+  // the first round reads only the parked coefficients; it waits for the previous
+  // block's tile store (which reads sm) only before writing sm itself, so its loads
+  // and butterflies overlap that store
+  if constexpr (r == TOP) __syncthreads();
+  rstore4<M, C, r, S0>(v, sm);
   __syncthreads();
   if constexpr (r > 0) {
 #pragma unroll
@@ -621,8 +625,7 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPa
       gf.gbase = ((q + 1) << (gi.a + M)) | gi.gbase;
     }
     fwd_rounds4<M, C, TOP>(sm, cf, gq, fwd.tw, t, gf, more);
-    tile_store4<M, C>(sm, dst, gq);
-    __syncthreads();
+    tile_store4<M, C>(sm, dst, gq);  // the next block's first round waits for it before writing sm
   }
 }
 
