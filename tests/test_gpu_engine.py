@@ -240,6 +240,24 @@ def test_engine_holds_at_most_the_budget(L):
     assert got == ref
 
 
+def test_engine_small_budget_gets_smaller_batches(L):
+    """A budget below a full batch workspace (64 proofs at log_n 16) still runs the
+    jobs, in smaller batches, with the same proofs."""
+    from vortexstark_b200 import api
+    job = api.fib_job(16, 1, 7)
+    with api.Engine(1) as probe:
+        full = probe.workspace_bytes(job)
+        tw = probe.stats()["twiddle_bytes"]
+    budget = full // 4 + tw + (16 << 20)
+    with api.Engine(2, budget) as eng:
+        small = eng.workspace_bytes(job)
+        assert small < full
+        jobs = [api.fib_job(16, 1, k) for k in range(6)]
+        res = [eng.wait(t)[0] for t in eng.submit_many(jobs)]
+        assert eng.stats()["peak_held_bytes"] <= budget
+    assert res == [api.prove_fib(1, k, 16) for k in range(6)]
+
+
 def test_engine_rejects_job_above_budget(L):
     from vortexstark_b200 import api
     with api.Engine(2, 1 << 20) as eng:

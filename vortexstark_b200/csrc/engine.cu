@@ -153,9 +153,14 @@ struct Engine {
   }
   int level_of(const vs_job& j) const { return by_size ? prio_level(class_bytes(j)) : kPrioLevels - 1; }
 
+  // Jobs per batch at a trace size: the default capacity (or the set limit), halved
+  // until the workspace fits the budget, so a small budget gets smaller batches
+  // instead of refused jobs.
   uint32_t batch_capacity(uint32_t log_n) const {
-    const uint32_t c = BatchProver::default_capacity(log_n);
-    return batch_limit ? std::min(c, batch_limit) : c;
+    uint32_t c = BatchProver::default_capacity(log_n);
+    if (batch_limit) c = std::min(c, batch_limit);
+    while (c > 1 && round2m(BatchProver::bytes_for(log_n, c)) > budget) c = (c + 1) / 2;
+    return c;
   }
   bool batched(const vs_job& j) const { return j.kind == VS_JOB_FIB && j.log_n >= 4 && j.log_n <= BATCH_MAX_LOG_N; }
 
