@@ -529,7 +529,7 @@ int vs_engine_wait_for(void* h, uint64_t ticket, double timeout_s, vs_job_result
   std::unique_lock<std::mutex> lk(e->mu);
   auto it = e->results.find(ticket);
   if (it == e->results.end()) return set_error(VS_ERR_INVALID, "unknown ticket %llu", (unsigned long long)ticket);
-  if (timeout_s < 0) {
+  if (timeout_s < 0 || timeout_s > 1e6) {  // no limit (longer limits would overflow the clock's range)
     e->cv_done.wait(lk, [&] { return it->second.done; });
   } else if (!e->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return it->second.done; })) {
     return set_error(VS_ERR_TIMEOUT, "job %llu not finished after %.3f s", (unsigned long long)ticket, timeout_s);
