@@ -433,16 +433,20 @@ def proof_workloads(args):
     # proves queued Fibonacci jobs of one size as one batch (one graph launch, one
     # kernel per stage for all of them); batch_limit 1 is one proof per launch.
     def batched(jobs, limit, warm):
-        with api.Engine(args.slots, size_priority=False) as eng:
+        """Median of three timed runs of the job list, after an untimed warm-up run that
+        creates the workspaces the runs use. The 120 GB budget bounds the cached
+        workspaces of 16 slots (the engine frees idle ones of other shapes as needed)."""
+        with api.Engine(args.batch_slots, 120 * 10**9, size_priority=False) as eng:
             eng.set_batch_limit(limit)
-            prep(eng, jobs)
             W.run_list(eng, jobs[:warm], sequential=False)
-            return W.run_list(eng, jobs, sequential=False)
+            runs = [W.run_list(eng, jobs, sequential=False) for _ in range(3)]
+        runs.sort(key=lambda x: x[0])
+        return runs[1]
 
     t_e, r_e = batched(plain, 0, len(plain))
-    t_1, r_1 = batched(plain, 1, 16)
-    out["batched_fib16"] = {"workload": "the same 64 proofs submitted at once to the slot engine",
-                            "slots": args.slots, "proofs_per_s": len(plain) / t_e,
+    t_1, r_1 = batched(plain, 1, len(plain))
+    out["batched_fib16"] = {"workload": "the same 64 proofs submitted at once to the slot engine (median of 3 runs)",
+                            "slots": args.batch_slots, "proofs_per_s": len(plain) / t_e,
                             "vs_plain": t_plain / t_e,
                             "one_proof_per_launch_proofs_per_s": len(plain) / t_1,
                             "identical_to_plain": all(x[0] == y for x, y in zip(r_e, r_plain)) and
@@ -456,11 +460,12 @@ def proof_workloads(args):
         prep(one, jobs)
         t_one, r_one = W.run_list(one, jobs, sequential=True)
     t_b, r_b = batched(jobs, 0, len(jobs))
-    t_b1, r_b1 = batched(jobs, 1, 8)
+    t_b1, r_b1 = batched(jobs, 1, len(jobs))
     n_fib = sum(1 for j in jobs if j.kind == api.FIB)
     out["batched_mix"] = {
-        "workload": "64 jobs, log_n U{16..22}: Fibonacci proofs (a1 seeded) or 1-34 seeded uniform columns (commit)",
-        "slots": args.slots, "jobs_per_s": len(jobs) / t_b, "proofs_per_s": n_fib / t_b,
+        "workload": "64 jobs, log_n U{16..22}: Fibonacci proofs (a1 seeded) or 1-34 seeded uniform columns (commit); "
+                    "median of 3 runs",
+        "slots": args.batch_slots, "jobs_per_s": len(jobs) / t_b, "proofs_per_s": n_fib / t_b,
         "plain_path_jobs_per_s": len(jobs) / t_p, "engine_one_slot_jobs_per_s": len(jobs) / t_one,
         "one_proof_per_launch_jobs_per_s": len(jobs) / t_b1,
         "vs_plain": t_p / t_b, "vs_one_slot": t_one / t_b,
@@ -575,7 +580,10 @@ def main():
     ap.add_argument("--no-oods", action="store_true", help="skip the OODS quotient kernels")
     ap.add_argument("--no-cairo", action="store_true", help="skip the Cairo trace commitment + tail chain")
     ap.add_argument("--cairo-log-n", type=int, default=22, help="trace rows (log) of the Cairo chain")
-    ap.add_argument("--slots", type=int, default=8, help="concurrent slots of the batched and served engines")
+    ap.add_argument("--slots", type=int, default=8, help="concurrent slots of the served engines")
+    ap.add_argument("--batch-slots", type=int, default=16,
+                    help="concurrent slots of the batched (throughput) engines: more batches in flight let "
+                         "one batch's host serialisation overlap another's kernels")
     ap.add_argument("--served-jobs", type=int, default=600)
     ap.add_argument("--no-autotune", action="store_true", help="keep the default NTT plans (no autotuning)")
     ap.add_argument("--merkle-split", type=int, default=None,
