@@ -409,6 +409,34 @@ struct Tile4 {
   static constexpr int R(int r) { return 3 * (r + 1) <= MC ? 3 : MC - 3 * r; }
 };
 
+// Whether chunk rounds r and r + 1 of a tile give every warp the same 16-byte
+// chunks, so that a warp barrier orders the two rounds: the warp bits of the thread
+// index (bits 5 and up) land on chunk bit b below the round and b + R above it in
+// ins4, and on chunk bit b + 3 in the word round of a C = 0 tile (32 consecutive
+// words per thread). (Checked against the address maps of every tile shape, for all
+// threads, on the CPU.) Tiles of fewer than 32 threads keep CTA barriers.
+template <int M, int C, int S0>
+__host__ __device__ constexpr bool warp_local_next(int r) {
+  using S = Tile4<M, C, S0>;
+  bool same = S::NT >= 32 && r + 1 < S::NR;
+  for (int b = 5; same && (1 << b) < S::NT; b++) {
+    const int fa = b < S::P0(r) - 2 ? b : b + S::R(r);
+    const int fb = b < S::P0(r + 1) - 2 ? b : b + S::R(r + 1);
+    same = fa == fb;
+  }
+  return same;
+}
+// The word round and chunk round 0 of a C = 0 tile (S0 = 5).
+template <int M>
+__host__ __device__ constexpr bool warp_local_word() {
+  using S = Tile4<M, 0, 5>;
+  return S::NT >= 32 && S::R(0) == 3;
+}
+__device__ __forceinline__ void round_sync(bool warp_local) {
+  if (warp_local) __syncwarp();
+  else __syncthreads();
+}
+
 // Word address of chunk k (R round bits at word bit P0) of chunk group o; o
 // enumerates the chunk-index bits outside the round.
 template <int P0, int R>
@@ -554,7 +582,9 @@ __device__ __forceinline__ void inv_rounds4(uint32_t* sm, uint32_t* cf, const Ti
   } else {
     rstore4<M, C, r, S0>(v, sm);
   }
-  __syncthreads();
+  // the forward pass's first round reads cf with the last round's own map (a warp
+  // barrier orders them; it waits for all warps before it overwrites sm)
+  round_sync(r == TOP ? Tile4<M, C, S0>::NT >= 32 : warp_local_next<M, C, S0>(r));
   if constexpr (r < TOP) {
 #pragma unroll
     for (int k = 0; k < 8; k++) t[k] = tn[k];
@@ -583,7 +613,7 @@ __device__ __forceinline__ void fwd_rounds4(uint32_t* sm, const uint32_t* cf, co
   // and butterflies overlap that store
   if constexpr (r == TOP) __syncthreads();
   rstore4<M, C, r, S0>(v, sm);
-  __syncthreads();
+  round_sync(r > 0 && warp_local_next<M, C, S0>(r - 1));  // round 0: the tile store reads everything
   if constexpr (r > 0) {
 #pragma unroll
     for (int k = 0; k < 8; k++) t[k] = tn[k];
@@ -699,21 +729,23 @@ __global__ void __launch_bounds__(1 << (M + C - 5), (M + C == 13) ? 3 : 2) ntt_p
     const TileGeo g = tile_geo<M, C>(p.a, w / n_cols);
     // (fetching a round's twiddles one round ahead, as the LDE top pass does,
     // measured slower here: the double-buffered tiles already hide the latency)
+    // warp barriers between rounds that give every warp the same chunks
+    // (warp_local_next, warp_local_word), CTA barriers elsewhere
     if (!FWD) {
       if (C == 0) {
         round_sm<false, M, C, 0>(sm, g, p.tw, 0);
-        __syncthreads();
+        round_sync(C == 0 && warp_local_word<(C == 0 ? M : 13)>());
       }
 #pragma unroll
       for (int r = 0; r < S4::NR; r++) {
         chunk_round<false, M, C, S0>(r, sm, g, p.tw, r == S4::NR - 1 ? p.scale : 0u);
-        __syncthreads();
+        round_sync(warp_local_next<M, C, S0>(r));  // false after the last round: the tile store follows
       }
     } else {
 #pragma unroll
       for (int r = S4::NR - 1; r >= 0; r--) {
         chunk_round<true, M, C, S0>(r, sm, g, p.tw, 0u);
-        __syncthreads();
+        round_sync(r > 0 ? warp_local_next<M, C, S0>(r - 1) : (C == 0 && warp_local_word<(C == 0 ? M : 13)>()));
       }
       if (C == 0) {
         round_sm<true, M, C, 0>(sm, g, p.tw, 0);
