@@ -81,7 +81,8 @@ def test_stwo_evaluate_interpolate(L, log_n):
     assert np.array_equal(host(d), x)
 
 
-@pytest.mark.parametrize("log_n,ncols", [(5, 1), (8, 3), (13, 2), (14, 2), (16, 5), (18, 2), (24, 1)])
+@pytest.mark.parametrize("log_n,ncols", [(5, 1), (8, 3), (13, 2), (14, 2), (16, 5), (18, 2), (22, 2), (23, 1),
+                                         (24, 1)])
 def test_lde_stwo(L, log_n, ncols):
     rng = np.random.default_rng(300 + log_n)
     cols = rand_m31(rng, ncols, 1 << log_n)
@@ -90,8 +91,8 @@ def test_lde_stwo(L, log_n, ncols):
     dst = empty(ncols * N)
     V.check(L.vs_lde_stwo(ptr(src), 1 << log_n, ptr(dst), N, ncols, log_n, 2, None), "vs_lde_stwo")
     out = host(dst).reshape(ncols, N)
-    if log_n <= 18:
-        assert np.array_equal(out, O.stwo_lde_columns(cols, log_n, 2, threads=4))
+    if log_n <= 23:
+        assert np.array_equal(out, O.stwo_lde_columns(cols, log_n, 2, threads=8))
     else:  # size-independent property: interpolating the LDE gives the trace coefficients zero-padded
         fwd, inv = O.stwo_twiddles(log_n + 2)
         d = dev(out[0])
@@ -105,7 +106,23 @@ def test_lde_stwo(L, log_n, ncols):
     assert np.array_equal(host(src).reshape(ncols, -1), cols)  # input untouched
 
 
-@pytest.mark.parametrize("log_n", [5, 9, 13, 16])
+@pytest.mark.parametrize("log_n,blowup", [(22, 1), (22, 3), (23, 1)])
+def test_lde_stwo_blowups(L, log_n, blowup):
+    """The LDE top pass at the trace sizes whose tile rows are 16-64 bytes (2^22 and
+    2^23: rows of 64 and 32 bytes, stored by bulk tensor stores) for blowups other
+    than 4, two columns at a padded column stride, against the oracle."""
+    rng = np.random.default_rng(700 + 10 * log_n + blowup)
+    ncols, n = 2, 1 << log_n
+    N = n << blowup
+    cols = rand_m31(rng, ncols, n)
+    stride = N + 64  # 64 words of padding between the evaluation columns
+    dst = empty(ncols * stride)
+    V.check(L.vs_lde_stwo(ptr(dev(cols.reshape(-1))), n, ptr(dst), stride, ncols, log_n, blowup, None), "vs_lde_stwo")
+    out = host(dst).reshape(ncols, stride)[:, :N]
+    assert np.array_equal(out, O.stwo_lde_columns(cols, log_n, blowup, threads=8))
+
+
+@pytest.mark.parametrize("log_n", [5, 9, 13, 16, 22])
 def test_lde_native(L, log_n):
     rng = np.random.default_rng(400 + log_n)
     x = rand_m31(rng, 1 << log_n)

@@ -26,7 +26,9 @@
 // of a zero-padded input only replicate the coefficients), so neither the
 // coefficients nor the zero padding touch HBM. Its upper-tile form works on
 // 16-byte chunks in three-layer rounds (128-bit shared-memory traffic, one
-// twiddle per chunk, 80 registers, three CTAs per SM).
+// twiddle per chunk, 80 registers, three CTAs per SM); with 16-byte tile rows it
+// runs as CTA pairs (thread-block clusters) that store whole 32-byte sectors by
+// reading each other's tiles through distributed shared memory.
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -437,6 +439,31 @@ __device__ __forceinline__ void round_sync(bool warp_local) {
   else __syncthreads();
 }
 
+// Thread-block cluster primitives (the LDE top pass's cluster form): split cluster
+// barrier (arrive with release, wait with acquire semantics at cluster scope) and
+// loads from a peer CTA's shared memory (distributed shared memory).
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// the same shared-memory offset in the CTA of cluster rank `rank`
+__device__ __forceinline__ uint32_t cluster_peer(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ uint4 ld_cluster16(uint32_t addr) {
+  uint4 v;
+  asm volatile("ld.shared::cluster.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(addr)
+               : "memory");
+  return v;
+}
+
 // Word address of chunk k (R round bits at word bit P0) of chunk group o; o
 // enumerates the chunk-index bits outside the round.
 template <int P0, int R>
@@ -462,6 +489,31 @@ __device__ __forceinline__ void tile_store4(const uint32_t* sm, uint32_t* __rest
   for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
     const uint32_t e = 4 * (threadIdx.x + i * S::NT);
     *reinterpret_cast<uint4*>(dst + gidx<M, C>(g, e)) = *reinterpret_cast<const uint4*>(sm + swz<0>(e));
+  }
+}
+// Tile store of a cluster of K CTAs over adjacent tiles lo0 .. lo0+K-1: each tile
+// holds 2^C consecutive words of every row, the K tiles together a segment of
+// K 2^C words (up to 128 bytes). CTA `rank` stores rows [rank R/K, (rank+1) R/K)
+// of all K tiles, reading the other tiles' pieces from their CTAs' shared memory,
+// so consecutive threads write whole segments (a tile alone can only store its
+// 2^C-word pieces: with 16-byte pieces, half sectors, one memory request each).
+// The caller brackets it with cluster barriers: every tile of the cluster is
+// complete before, and no CTA overwrites its tile until all have read it.
+template <int M, int C, int K>
+__device__ __forceinline__ void tile_store4_cluster(const uint32_t* sm, uint32_t* __restrict__ dst, const TileGeo& g) {
+  using S = Tile<M, C>;
+  static_assert(C >= 2 && (K << C) <= 32, "a cluster covers at most one 128-byte line of every row");
+  constexpr uint32_t R = 1u << M, CH = 1u << (C - 2), SEG = K * CH;  // rows; 16-byte chunks per tile row, per segment
+  const uint32_t rank = cluster_rank();
+  const uint32_t base = g.gbase - (rank << C);  // the cluster's first tile: lo0 << C
+  const uint32_t sm0 = smem_addr(sm);
+#pragma unroll 4
+  for (int i = 0; i < S::SIZE / 4 / S::NT; i++) {
+    const uint32_t p = threadIdx.x + i * S::NT;  // chunk of this CTA's share
+    const uint32_t j = p % SEG, r = rank * (R / K) + p / SEG;
+    const uint32_t e = (r << C) | ((j % CH) << 2);  // tile word of chunk j % CH of row r
+    const uint4 v = ld_cluster16(cluster_peer(sm0 + 4 * swz<0>(e), j / CH));
+    *reinterpret_cast<uint4*>(dst + (base | (r << g.a) | (j << 2))) = v;
   }
 }
 
@@ -594,7 +646,7 @@ __device__ __forceinline__ void inv_rounds4(uint32_t* sm, uint32_t* cf, const Ti
 // Forward chunk rounds r..0 (round TOP reads from cf: the parked coefficients of
 // the LDE top pass, the working tile in a pass kernel), twiddles fetched one round
 // ahead as above.
-template <int M, int C, int r, int S0 = C>
+template <int M, int C, int r, int S0 = C, int K = 1>
 __device__ __forceinline__ void fwd_rounds4(uint32_t* sm, const uint32_t* cf, const TileGeo& g, const NttTw& tw,
                                             uint32_t (&t)[8], const TileGeo& gn, bool next) {
   constexpr int TOP = Tile4<M, C, S0>::NR - 1;
@@ -611,13 +663,23 @@ __device__ __forceinline__ void fwd_rounds4(uint32_t* sm, const uint32_t* cf, co
   // the first round reads only the parked coefficients; it waits for the previous
   // block's tile store (which reads sm) only before writing sm itself, so its loads
   // and butterflies overlap that store
-  if constexpr (r == TOP) __syncthreads();
+  // (in a cluster: until every CTA of the cluster has stored its share, which reads
+  // this tile too)
+  if constexpr (r == TOP) {
+    if constexpr (K > 1) cluster_wait();
+    else __syncthreads();
+  }
   rstore4<M, C, r, S0>(v, sm);
-  round_sync(r > 0 && warp_local_next<M, C, S0>(r - 1));  // round 0: the tile store reads everything
+  if constexpr (K > 1 && r == 0) {  // the cluster's tile store reads every tile of the cluster
+    cluster_arrive();
+    cluster_wait();
+  } else {
+    round_sync(r > 0 && warp_local_next<M, C, S0>(r - 1));  // round 0: the tile store reads everything
+  }
   if constexpr (r > 0) {
 #pragma unroll
     for (int k = 0; k < 8; k++) t[k] = tn[k];
-    fwd_rounds4<M, C, (r > 0 ? r - 1 : 0), S0>(sm, cf, g, tw, t, gn, next);
+    fwd_rounds4<M, C, (r > 0 ? r - 1 : 0), S0, K>(sm, cf, g, tw, t, gn, next);
   }
 }
 
@@ -627,7 +689,16 @@ __device__ __forceinline__ void fwd_rounds4(uint32_t* sm, const uint32_t* cf, co
 // Each round's twiddles are loaded during the round before it (the first inverse
 // round's during the tile load, a block's first forward round's during the
 // previous block's tile store), so their L2 latency is off the round's critical path.
-template <int M, int C>
+//
+// Cluster form (K > 1, launched as clusters of K CTAs over adjacent tiles): the
+// blocks' tiles are stored as segments of K 2^C words gathered across the cluster
+// (tile_store4_cluster) instead of 2^C-word pieces. The split cluster barrier
+// alternates arrive and wait on every thread: an arrive after the inverse rounds;
+// per block, a wait before the first round writes
+// the tile (every CTA has finished reading the previous block's tiles), an arrive
+// and wait after the last round (all tiles complete), an arrive after the store;
+// and a last wait before exit, so no CTA leaves while its tile is still being read.
+template <int M, int C, int K = 1>
 __global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPass inv, NttPass fwd, uint32_t B) {
   using S = Tile4<M, C>;
   static_assert(S::NR <= 4, "at most four chunk rounds");
@@ -647,6 +718,7 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPa
   // each block's first-round twiddles are fetched right after the butterflies of
   // the round before it (the last inverse round, then each block's round 0)
   inv_rounds4<M, C, 0>(sm, cf, gi, inv.tw, inv.scale, t, gf, fwd.tw);
+  if constexpr (K > 1) cluster_arrive();
   for (uint32_t q = 0; q < (1u << B); q++) {
     const TileGeo gq = gf;
     const bool more = q + 1 < (1u << B);
@@ -654,9 +726,16 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPa
       gf.hi = q + 1;
       gf.gbase = ((q + 1) << (gi.a + M)) | gi.gbase;
     }
-    fwd_rounds4<M, C, TOP>(sm, cf, gq, fwd.tw, t, gf, more);
-    tile_store4<M, C>(sm, dst, gq);  // the next block's first round waits for it before writing sm
+    fwd_rounds4<M, C, TOP, C, K>(sm, cf, gq, fwd.tw, t, gf, more);
+    // the next block's first round waits for the store before writing sm
+    if constexpr (K > 1) {
+      tile_store4_cluster<M, C, K>(sm, dst, gq);
+      cluster_arrive();
+    } else {
+      tile_store4<M, C>(sm, dst, gq);
+    }
   }
+  if constexpr (K > 1) cluster_wait();
 }
 
 // One chunk round of a pass: shared-memory loads, then the round's twiddles, then
@@ -767,6 +846,14 @@ template <bool FWD, int M> PassFn pass4_lo() { return ntt_pass4_kernel<FWD, M, 0
 template <bool FWD, int M> PassFn pass4_hi() { return ntt_pass4_kernel<FWD, M, 13 - M>; }
 template <int M> TopFn top_lo() { return ntt_lde_top_kernel<M, 0>; }
 template <int M> TopFn top_hi() { return ntt_lde_top4_kernel<M, 13 - M>; }
+// The LDE top pass over M = 11 layers (tiles of 16-byte rows, traces of 2^24) runs
+// as CTA pairs, which store whole 32-byte sectors. Measured on 34 x 2^24: LDE 16.31
+// ms with single CTAs, 15.24 with pairs, 15.87 with clusters of 4 and 17.4 with 8
+// (whole 128-byte lines, but every block waits for 8 CTAs). Rows of 32 and 64 bytes
+// (M = 10, 9) are whole sectors already: pairs there measured slower (2^23: 7.23 ->
+// 7.34 ms, 2^22: 3.32 -> 3.56 ms).
+constexpr int kTopPair = 2;
+TopFn top_hi_pair() { return ntt_lde_top4_kernel<11, 2, kTopPair>; }
 template <int M> TopFn top5_hi() { return ntt_lde_top_kernel<M, 13 - M>; }
 
 static PassFn pass_fn(bool fwd, uint32_t M, uint32_t C) {
@@ -1186,8 +1273,34 @@ static int ntt_lde_aligned(const NttColumns& io, uint32_t l, uint32_t B, const N
     TopFn fn = top_fn(M, r.c, plan.radix);
     if (!fn) return set_error(VS_ERR_INVALID, "ntt: no LDE kernel for shape M=%u C=%u", M, r.c);
     const uint32_t smem = 8u << T;  // working tile + coefficient tile
-    VS_TRY(allow_smem((const void*)fn, smem));
-    fn<<<dim3(1u << (l - T), io.n_cols), 1u << (T - 5), smem, st>>>(pi, pf, B);
+    const dim3 grid(1u << (l - T), io.n_cols), block(1u << (T - 5));
+    // 16-byte-row tiles run as CTA pairs (whole-sector tile stores); if the
+    // cluster launch is refused, the plain kernel runs instead
+    TopFn cfn = nullptr;
+    const uint32_t K = kTopPair;
+    if (plan.radix != 5 && M == 11 && r.c == 2) cfn = top_hi_pair();
+    bool launched = false;
+    if (cfn && grid.x % K == 0) {
+      VS_TRY(allow_smem((const void*)cfn, smem));
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = grid;
+      cfg.blockDim = block;
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = st;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = K;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      if (cudaLaunchKernelEx(&cfg, cfn, pi, pf, B) == cudaSuccess) launched = true;
+      else cudaGetLastError();  // clear the refused launch's error
+    }
+    if (!launched) {
+      VS_TRY(allow_smem((const void*)fn, smem));
+      fn<<<grid, block, smem, st>>>(pi, pf, B);
+    }
     VS_LAUNCHED("ntt_lde_top_kernel");
   }
   // 3. forward passes below the top one over the whole evaluation domain
