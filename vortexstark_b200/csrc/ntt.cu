@@ -443,6 +443,13 @@ __device__ __forceinline__ void round_sync(bool warp_local) {
 // barrier (arrive with release, wait with acquire semantics at cluster scope) and
 // loads from a peer CTA's shared memory (distributed shared memory).
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+// Arrive without release semantics (it does not wait for the thread's outstanding
+// stores): for arrivals that only announce that the thread's reads are complete,
+// which program order already guarantees when each loaded value has been consumed
+// by an instruction before the arrive.
+__device__ __forceinline__ void cluster_arrive_relaxed() {
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
 __device__ __forceinline__ uint32_t cluster_rank() {
   uint32_t r;
@@ -657,7 +664,8 @@ __device__ __forceinline__ void fwd_rounds4(uint32_t* sm, const uint32_t* cf, co
   rbfly4_t<true, M, C, r, S0>(v, t);
   // after the block's last butterflies t is free: fetch the next block's
   // first-round twiddles into it, ahead of the stores, barrier and tile store
-  if constexpr (r == 0) {
+  // (in a cluster: after the release arrive below, which would wait for these loads)
+  if constexpr (r == 0 && K == 1) {
     if (next) tw4_fetch<M, C, TOP, S0>(t, gn, tw);
   }
   // the first round reads only the parked coefficients; it waits for the previous
@@ -672,6 +680,7 @@ __device__ __forceinline__ void fwd_rounds4(uint32_t* sm, const uint32_t* cf, co
   rstore4<M, C, r, S0>(v, sm);
   if constexpr (K > 1 && r == 0) {  // the cluster's tile store reads every tile of the cluster
     cluster_arrive();
+    if (next) tw4_fetch<M, C, TOP, S0>(t, gn, tw);
     cluster_wait();
   } else {
     round_sync(r > 0 && warp_local_next<M, C, S0>(r - 1));  // round 0: the tile store reads everything
@@ -696,7 +705,8 @@ __device__ __forceinline__ void fwd_rounds4(uint32_t* sm, const uint32_t* cf, co
 // alternates arrive and wait on every thread: an arrive after the inverse rounds;
 // per block, a wait before the first round writes
 // the tile (every CTA has finished reading the previous block's tiles), an arrive
-// and wait after the last round (all tiles complete), an arrive after the store;
+// and wait after the last round (all tiles complete; the arrive releases the tile
+// to the other CTAs), an arrive after the store (relaxed: it only announces reads);
 // and a last wait before exit, so no CTA leaves while its tile is still being read.
 template <int M, int C, int K = 1>
 __global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPass inv, NttPass fwd, uint32_t B) {
@@ -718,7 +728,7 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPa
   // each block's first-round twiddles are fetched right after the butterflies of
   // the round before it (the last inverse round, then each block's round 0)
   inv_rounds4<M, C, 0>(sm, cf, gi, inv.tw, inv.scale, t, gf, fwd.tw);
-  if constexpr (K > 1) cluster_arrive();
+  if constexpr (K > 1) cluster_arrive_relaxed();  // this CTA's last reads of sm are consumed
   for (uint32_t q = 0; q < (1u << B); q++) {
     const TileGeo gq = gf;
     const bool more = q + 1 < (1u << B);
@@ -730,7 +740,9 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPa
     // the next block's first round waits for the store before writing sm
     if constexpr (K > 1) {
       tile_store4_cluster<M, C, K>(sm, dst, gq);
-      cluster_arrive();
+      // every value read from the cluster's tiles is already stored, so the reads
+      // are complete; no release (it would wait for those global stores)
+      cluster_arrive_relaxed();
     } else {
       tile_store4<M, C>(sm, dst, gq);
     }
