@@ -106,11 +106,12 @@ def test_lde_stwo(L, log_n, ncols):
     assert np.array_equal(host(src).reshape(ncols, -1), cols)  # input untouched
 
 
-@pytest.mark.parametrize("log_n,blowup", [(22, 1), (22, 3), (23, 1)])
+@pytest.mark.parametrize("log_n,blowup", [(22, 1), (22, 3), (23, 1), (24, 1)])
 def test_lde_stwo_blowups(L, log_n, blowup):
-    """The LDE top pass at the trace sizes whose tile rows are 16-64 bytes (2^22 and
-    2^23: rows of 64 and 32 bytes, stored by bulk tensor stores) for blowups other
-    than 4, two columns at a padded column stride, against the oracle."""
+    """The LDE top pass at the trace sizes whose tile rows are 16-64 bytes (2^24, 2^23
+    and 2^22: rows of 16, 32 and 64 bytes; the 16-byte rows run as CTA pairs that
+    store whole sectors) for blowups other than 4, two columns at a padded column
+    stride, against the oracle."""
     rng = np.random.default_rng(700 + 10 * log_n + blowup)
     ncols, n = 2, 1 << log_n
     N = n << blowup
