@@ -84,10 +84,16 @@ def workload(args):
 
 def config_json(args):
     n_cols, log_n, blow, fri_log, N, _ = workload(args)
+    cols_gb, lde_gb, fri_gb = n_cols * 4 * (1 << log_n) / 1e9, n_cols * 4 * N / 1e9, 16 * (1 << fri_log) / 1e9
+    l2_gb = 0.126
+    big = cols_gb > l2_gb and fri_gb > l2_gb
     return {"workload": f"commitment layer: {n_cols} cols x 2^{log_n} rows, stwo LDE x{1 << blow} + row-packed "
                         f"Blake2s root, then FRI fold+commit of 2^{fri_log} QM31",
             "n_cols": n_cols, "log_n": log_n, "blowup": 1 << blow, "fri_log_n": fri_log,
-            "l2": "inputs larger than L2 (2.2 GB columns, 1 GB QM31 vector)", "seed": hex(SEED)}
+            "l2": (f"inputs larger than L2 ({cols_gb:.2f} GB columns, {lde_gb:.2f} GB LDE, {fri_gb:.2f} GB QM31 "
+                   f"vector; no flush between steps)" if big else
+                   f"inputs not all larger than the 126 MB L2 ({cols_gb:.3f} GB columns, {fri_gb:.3f} GB QM31 vector)"),
+            "seed": hex(SEED)}
 
 
 # ---------------------------------------------------------------- clocks
