@@ -123,6 +123,21 @@ def test_lde_stwo_blowups(L, log_n, blowup):
     assert np.array_equal(out, O.stwo_lde_columns(cols, log_n, blowup, threads=8))
 
 
+@pytest.mark.parametrize("log_n", [5, 13, 14, 20, 24])
+@pytest.mark.parametrize("native", [False, True])
+def test_lde_blowup_one_is_identity(L, log_n, native):
+    """An LDE onto the trace's own domain (blowup bits 0) interpolates and evaluates
+    on the same domain: it returns its input, bit for bit (the oracle does the same),
+    at every pass structure up to the 2^24 top pass run as CTA pairs."""
+    rng = np.random.default_rng(900 + log_n)
+    ncols, n = 2, 1 << log_n
+    cols = rand_m31(rng, ncols, n)
+    dst = empty(ncols * n)
+    fn = L.vs_lde_native if native else L.vs_lde_stwo
+    V.check(fn(ptr(dev(cols.reshape(-1))), n, ptr(dst), n, ncols, log_n, 0, None), "lde")
+    assert np.array_equal(host(dst).reshape(ncols, n), cols)
+
+
 @pytest.mark.parametrize("log_n", [5, 9, 13, 16, 22])
 def test_lde_native(L, log_n):
     rng = np.random.default_rng(400 + log_n)
