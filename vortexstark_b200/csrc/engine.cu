@@ -6,8 +6,9 @@
 // policy a quarter of the slots take only small jobs, oldest first) together with
 // the queued Fibonacci jobs of the same trace size, up to the batch capacity of
 // that size, and runs them as one batched proof (one graph launch, one kernel per
-// stage for all of them). It needs a workspace of the job's shape: an idle cached
-// one, or a new one when the device memory the engine holds stays within the HBM
+// stage for all of them). It needs a workspace of the job's shape (for a batch,
+// one that holds at least its proofs): an idle cached one, or a new one (a batch's
+// sized to the batch) when the device memory the engine holds stays within the HBM
 // budget. The held memory is every cached workspace, idle or in use, plus the
 // library's twiddle tables on the device (and the tables the new shape would
 // build). When a new workspace does not fit, idle workspaces of other shapes are
@@ -219,6 +220,28 @@ struct Engine {
             (!s.small_only || prio_level(class_bytes(o)) == 0))
           p.picks.push_back(it);
       }
+      // The batch runs in the smallest idle workspace of its size that holds it,
+      // else in a new one sized to the batch (the next power of two, up to the
+      // capacity), so slots that share a burst of small proofs do not each hold a
+      // full-capacity workspace: 16 slots running batches of 4 log_n 16 proofs hold
+      // 16 x 53 MB instead of 16 x 0.85 GB (throughput the same within run-to-run
+      // noise, 8.9-9.4 k proofs/s). Prepared workspaces (full capacity) serve
+      // every batch size.
+      const uint32_t n_picks = (uint32_t)p.picks.size();
+      size_t best = SIZE_MAX;
+      for (size_t i = 0; i < idle.size(); i++) {
+        const uint64_t k = idle[i]->key;
+        if ((k >> 32) != (p.key >> 32) || (uint32_t)k < n_picks) continue;
+        if (best == SIZE_MAX || (uint32_t)k < (uint32_t)idle[best]->key) best = i;
+      }
+      if (best != SIZE_MAX) {
+        p.key = idle[best]->key;
+        p.idle_at = best;
+        return true;
+      }
+      uint32_t want = 1;
+      while (want < n_picks) want <<= 1;
+      p.key = ws_key(WS_BATCH, j.log_n, std::min(batch_capacity(j.log_n), want));
     }
     for (size_t i = 0; i < idle.size(); i++)
       if (idle[i]->key == p.key) { p.idle_at = i; return true; }
