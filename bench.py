@@ -645,7 +645,10 @@ def main():
     if not args.no_autotune:
         tuning = {}
         for tl in sorted(set(args.tune_sizes) | {args.log_n}):
-            default = api.ntt_plan(tl)
+            lo, items, radix = api.ntt_plan(tl)
+            # the default's items (0) as the candidate it equals: one tile per CTA in
+            # 13-layer lower passes, 8 tiles per CTA otherwise
+            default = (lo, items or (1 if lo == 13 else 8), radix)
             r = api.autotune_lde(tl, n_cols=args.cols, blowup=2, reps=3)
             times = dict(r["candidates"])
             tuning[str(tl)] = {"plan": list(r["best"]), "ms": times[tuple(r["best"])],

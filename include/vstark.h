@@ -241,7 +241,9 @@ int vs_lde_native(const uint32_t* d_src, uint64_t src_stride, uint32_t* d_dst, u
  *   lower      layers of the first (lower) pass; 14 <= log_n <= 24 accepts
  *              max(5, log_n - 11) .. 13, other sizes only their default
  *              (13, or log_n below 14);
- *   items      tiles a pass CTA transforms before it retires, 1..64 (0: 8);
+ *   items      tiles a pass CTA transforms before it retires, 1..64; 1 runs 13-layer
+ *              lower passes in a single-buffered kernel (four CTAs per SM, one
+ *              tile each); 0: the default (1 for 13-layer lower passes, 8 elsewhere);
  *   radix      layers per register round above a C = 0 tile's first five:
  *              3 (16-byte chunk rounds, the default) or 5 (word rounds); 0: default.
  *              The LDE of at most 13 layers has the word-round form only.

@@ -17,25 +17,26 @@ def test_candidates_shape():
         cands = api.ntt_plan_candidates(log_n)
         assert cands and len(set(cands)) == len(cands)
         for lower, items, radix in cands:
-            assert items in (4, 8, 16)
+            assert items in (1, 4, 8, 16)
             if log_n <= 13:
                 assert (lower, radix) == (log_n, 3)
             else:
                 assert radix in (3, 5)
                 assert 10 <= lower <= 13 and log_n - lower <= 11 if log_n <= 24 else lower == 13
-    assert len(api.ntt_plan_candidates(20)) == 4 * 3 * 2  # lower 10..13 x items x radix
-    assert len(api.ntt_plan_candidates(24)) == 6
+    assert len(api.ntt_plan_candidates(20)) == 4 * 4 * 2  # lower 10..13 x items x radix
+    assert len(api.ntt_plan_candidates(24)) == 8
 
 
 def test_set_get_round_trip_and_defaults():
-    assert api.ntt_plan(24) == (13, 8, 3)
-    assert api.ntt_plan(12) == (12, 8, 3)
+    # items 0: the default (one tile per CTA in 13-layer lower passes, 8 elsewhere)
+    assert api.ntt_plan(24) == (13, 0, 3)
+    assert api.ntt_plan(12) == (12, 0, 3)
     for log_n in (8, 14, 20, 24, 28):
         for plan in api.ntt_plan_candidates(log_n):
             api.set_ntt_plan(log_n, *plan)
             assert api.ntt_plan(log_n) == tuple(plan)
         api.set_ntt_plan(log_n)
-    assert api.ntt_plan(20) == (13, 8, 3)
+    assert api.ntt_plan(20) == (13, 0, 3)
 
 
 @pytest.mark.parametrize("log_n,plan", [(24, (12, 8, 3)), (20, (8, 8, 3)), (12, (10, 8, 5)), (28, (12, 8, 3)),

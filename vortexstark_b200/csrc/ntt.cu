@@ -848,6 +848,48 @@ __global__ void __launch_bounds__(1 << (M + C - 5), (M + C == 13) ? 3 : 2) ntt_p
   }
 }
 
+// Single-buffered form of ntt_pass4_kernel: one tile per CTA, half the shared
+// memory and at most 64 registers, so four CTAs share an SM instead of three (the
+// other CTAs' work hides a tile's load instead of the double buffer). Used for the
+// 13-layer lower passes when a plan asks for one tile per CTA (the default there):
+// LDE of 34 x 2^24 14.87 -> 14.72 ms, of 34 x 2^22 3.32 -> 3.25 ms.
+template <bool FWD, int M, int C>
+__global__ void __launch_bounds__(1 << (M + C - 5), 4) ntt_pass4s_kernel(NttPass p, uint32_t n_cols, uint32_t total) {
+  constexpr int S0 = C == 0 ? 5 : C;
+  using S4 = Tile4<M, C, S0>;
+  extern __shared__ __align__(16) uint32_t pass4s_sm[];
+  const uint32_t w = blockIdx.x;
+  if (w >= total) return;
+  uint32_t* sm = pass4s_sm;
+  const TileGeo g = tile_geo<M, C>(p.a, w / n_cols);
+  tile_load_async4<M, C>(sm, col_src(p, w % n_cols), g, p.src_mask);
+  cp_async_commit();
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+  if (!FWD) {
+    if (C == 0) {
+      round_sm<false, M, C, 0>(sm, g, p.tw, 0);
+      round_sync(C == 0 && warp_local_word<(C == 0 ? M : 13)>());
+    }
+#pragma unroll
+    for (int r = 0; r < S4::NR; r++) {
+      chunk_round<false, M, C, S0>(r, sm, g, p.tw, r == S4::NR - 1 ? p.scale : 0u);
+      round_sync(warp_local_next<M, C, S0>(r));
+    }
+  } else {
+#pragma unroll
+    for (int r = S4::NR - 1; r >= 0; r--) {
+      chunk_round<true, M, C, S0>(r, sm, g, p.tw, 0u);
+      round_sync(r > 0 ? warp_local_next<M, C, S0>(r - 1) : (C == 0 && warp_local_word<(C == 0 ? M : 13)>()));
+    }
+    if (C == 0) {
+      round_sm<true, M, C, 0>(sm, g, p.tw, 0);
+      __syncthreads();
+    }
+  }
+  tile_store4<M, C>(sm, col_dst(p, w % n_cols), g);
+}
+
 // Launch tables: single / lower passes use C = 0 (T = M, 5 <= M <= 13); upper
 // passes use T = 13 (C = 13 - M, 1 <= M <= 11).
 using PassFn = void (*)(NttPass, uint32_t, uint32_t);
@@ -961,7 +1003,8 @@ NttPlan ntt_plan(uint32_t L) {
     std::lock_guard<std::mutex> lk(g_plan_mu);
     p = g_plan[L];
   }
-  if (!p.items) p.items = 8;
+  // items stays 0 for the default: one tile per CTA in 13-layer lower passes (the
+  // single-buffered kernel), 8 elsewhere
   if (!p.radix) p.radix = 3;
   return p;
 }
@@ -980,7 +1023,7 @@ std::vector<NttPlan> ntt_plan_candidates(uint32_t L) {
   const bool upper_tile = L > kMaxT;  // the LDE top pass runs on C >= 2 tiles only above 13 layers
   const std::vector<uint32_t> radices = upper_tile ? std::vector<uint32_t>{3u, 5u} : std::vector<uint32_t>{0u};
   for (uint32_t lo : lowers)
-    for (uint32_t items : {4u, 8u, 16u})
+    for (uint32_t items : {1u, 4u, 8u, 16u})
       for (uint32_t radix : radices) v.push_back({lo == kMaxT ? 0u : lo, items, radix});
   return v;
 }
@@ -1041,6 +1084,15 @@ static uint32_t persistent_grid(const void* fn, uint32_t threads, uint32_t smem)
 
 static int launch_pass(NttPass p, bool fwd, uint32_t n_cols, cudaStream_t st) {
   const uint32_t M = p.b - p.a + 1, T = M + p.c;
+  if (p.radix != 5 && p.c == 0 && M == kMaxT && p.items <= 1) {  // one tile per CTA: single-buffered kernel
+    PassFn f = fwd ? ntt_pass4s_kernel<true, kMaxT, 0> : ntt_pass4s_kernel<false, kMaxT, 0>;
+    const uint64_t tot = (uint64_t)n_cols << (p.log_n - T);
+    if (tot > 0xFFFFFFFFull) return set_error(VS_ERR_INVALID, "ntt: %llu tiles", (unsigned long long)tot);
+    VS_TRY(allow_smem((const void*)f, 4u << T));
+    f<<<(uint32_t)tot, 1u << (T - 5), 4u << T, st>>>(p, n_cols, (uint32_t)tot);
+    VS_LAUNCHED("ntt_pass_kernel");
+    return VS_OK;
+  }
   PassFn fn = p.radix == 5 ? nullptr : pass4_fn(fwd, M, p.c);
   if (!fn) fn = pass_fn(fwd, M, p.c);
   if (!fn) return set_error(VS_ERR_INVALID, "ntt: no kernel for pass shape M=%u C=%u", M, p.c);
@@ -1631,7 +1683,7 @@ int vs_autotune_lde(uint32_t log_n, uint32_t n_cols, uint32_t blowup_bits, uint3
   if (dst) cudaFreeAsync(dst, st);
   if (rc != VS_OK) return rc;
   best[0] = best_plan.lower ? best_plan.lower : std::min<uint32_t>(log_n, kMaxT);
-  best[1] = best_plan.items ? best_plan.items : 8u;
+  best[1] = best_plan.items;  // 0: the default
   best[2] = best_plan.radix ? best_plan.radix : 3u;
   return check_cuda(cudaStreamSynchronize(st), "vs_autotune_lde");
 }
