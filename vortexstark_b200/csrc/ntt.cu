@@ -708,6 +708,9 @@ __device__ __forceinline__ void fwd_rounds4(uint32_t* sm, const uint32_t* cf, co
 // and wait after the last round (all tiles complete; the arrive releases the tile
 // to the other CTAs), an arrive after the store (relaxed: it only announces reads);
 // and a last wait before exit, so no CTA leaves while its tile is still being read.
+template <int M, int C>
+__device__ __forceinline__ void tile_load_async4(uint32_t* sm, const uint32_t* __restrict__ src, const TileGeo& g,
+                                                 uint32_t mask);
 template <int M, int C, int K = 1>
 __global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPass inv, NttPass fwd, uint32_t B) {
   using S = Tile4<M, C>;
@@ -718,8 +721,12 @@ __global__ void __launch_bounds__(1 << (M + C - 5), 3) ntt_lde_top4_kernel(NttPa
   uint32_t* cf = lde4_sm + S::SIZE;  // coefficients
   const TileGeo gi = tile_geo<M, C>(inv.a, blockIdx.x);
   uint32_t t[8];
+  // the input tile streams into shared memory by 16-byte cp.async (no registers in
+  // flight) while the first round's twiddles load
+  tile_load_async4<M, C>(sm, col_src(inv, blockIdx.y), gi, inv.src_mask);
+  cp_async_commit();
   tw4_fetch<M, C, 0>(t, gi, inv.tw);
-  tile_load4<M, C>(sm, col_src(inv, blockIdx.y), gi, inv.src_mask);
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   uint32_t* dst = col_dst(fwd, blockIdx.y);
   TileGeo gf = gi;
