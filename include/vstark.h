@@ -372,7 +372,8 @@ int vs_engine_create(uint32_t n_slots, uint64_t hbm_budget_bytes, void** engine)
 #define VS_ENGINE_FIFO_PRIORITY 1u
 int vs_engine_create_ex(uint32_t n_slots, uint64_t hbm_budget_bytes, uint32_t flags, void** engine);
 int vs_engine_destroy(void* engine);
-/* Builds the workspace for this job shape in every slot (outside any timing). */
+/* Builds the workspace for this job shape in every slot (outside any timing; for
+ * batched Fibonacci sizes a full-capacity one, which serves batches of any size). */
 int vs_engine_prepare(void* engine, const vs_job* shape);
 int vs_engine_submit(void* engine, const vs_job* job, uint64_t* ticket);
 /* Queues n jobs at once (all or none), so slots see them together and batch
@@ -396,8 +397,9 @@ double vs_engine_now(void* engine);
 /* At most max_jobs proofs per batch (0 = each size's default capacity, 1 = one
  * proof per graph launch). Takes effect for workspaces created afterwards. */
 int vs_engine_set_batch_limit(void* engine, uint32_t max_jobs);
-/* Device bytes of the workspace a job of this shape runs in (a batch workspace
- * for small Fibonacci proofs), not counting twiddle tables. */
+/* Device bytes of the largest workspace a job of this shape runs in (for small
+ * Fibonacci proofs the full-capacity batch workspace; a batch that finds no idle
+ * workspace gets one sized to it, at most this), not counting twiddle tables. */
 int vs_engine_workspace_bytes(void* engine, const vs_job* shape, uint64_t* bytes);
 /* Host-side fault injection for tests: the next `count` workspace creations fail
  * with VS_ERR_OOM before allocating anything; the engine stays usable. */
