@@ -84,8 +84,9 @@ int vs_fri_fold_commit(const uint32_t* d_src, uint32_t log_n, const uint32_t* h_
   uint32_t* scratch = nullptr;
   VS_CUDA(cudaMallocAsync((void**)&scratch, (merkle_scratch_words_any(N / 2) + 8) * 4, st));
   // FRI layer trees are fastest at a split of at most 5 (34 x 2^24 step: FRI 6.68 ms
-  // at split 0, 6.09 at 5, 6.22 at 8, the row-packed root's tuned value); the roots
-  // are the same for every split
+  // at split 0, 6.09 at 5, 6.22 at 8, the row-packed root's tuned value; this fold +
+  // commit of 2^26 alone: 6.59 / 6.44 / 6.35 / 6.28 / 6.30 / 6.31 / 6.38 ms at splits
+  // 2..8); the roots are the same for every split
   const uint32_t split = std::min<uint32_t>(merkle_split(), 5);
   const uint32_t* src[4] = {d_src, d_src + N, d_src + 2 * N, d_src + 3 * N};
   uint32_t* bufs[2] = {d_work, d_work + 2 * N};  // each holds 4 planes of <= N/2 words
