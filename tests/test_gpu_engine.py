@@ -142,6 +142,33 @@ def _occupy_then_submit(eng, jobs, log_n_block=18):
     return first, [eng.submit(j) for j in jobs]
 
 
+def test_batch_workspace_sized_to_batch(L):
+    """A batch that finds no idle workspace of its size gets one sized to it (the
+    next power of two of its proofs), far below the full-capacity workspace; a
+    prepared full-capacity workspace serves a batch of any size, so nothing new is
+    created for it. Results are the oracle's either way."""
+    from vortexstark_b200 import api
+    jobs = [api.fib_job(12, 1, k) for k in range(3)]
+    expected = [O.prove(1, k, 12) for k in range(3)]
+    block = api.commit_job(18, 34, 0x77)
+    with api.Engine(1) as eng:
+        full = eng.workspace_bytes(jobs[0])
+        commit_bytes = eng.workspace_bytes(block)
+        first, ts = _occupy_then_submit(eng, jobs)
+        eng.wait(first)
+        assert [eng.wait(t)[0] for t in ts] == expected
+        st = eng.stats()
+    assert st["workspaces_created"] == 2  # the blocking commitment's and the batch's
+    assert st["resident_bytes"] - commit_bytes < full // 4  # a workspace for 4 proofs, not 64
+    with api.Engine(1) as eng:
+        eng.prepare(jobs[0])
+        created = eng.stats()["workspaces_created"]
+        first, ts = _occupy_then_submit(eng, jobs)
+        eng.wait(first)
+        assert [eng.wait(t)[0] for t in ts] == expected
+        assert eng.stats()["workspaces_created"] == created + 1  # only the commitment's
+
+
 @pytest.mark.parametrize("log_n", [4, 7, 10, 13])
 def test_batched_proofs_match_oracle_and_plain(L, log_n):
     """Jobs of one size queued together run as one batch (one graph launch); every
